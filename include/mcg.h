@@ -1,0 +1,257 @@
+/*
+ * mcg.h - C ABI of the B200 D3Q27 colour-gradient lattice Boltzmann step.
+ *
+ * This is the drop-in boundary for the per-time-step path of
+ * Felipe-Aristi/Multicomponent_Color_Gradient.  That project has no FFI: its
+ * de-facto operator boundary is the launcher set in launch.cuh:13-118 plus the
+ * device-memory helpers in memory.cuh:58-133 and the mean-field runtime in
+ * meanF/meanFieldsRT.cuh:132-381.  Each entry point below names the reference
+ * interface it replaces.
+ *
+ * Conventions (kept identical to the reference so host buffers interoperate):
+ *   - NX*NY*NZ counts the one-cell ghost shell (utilities/bounds.cuh:6-13);
+ *   - node index id = x + NX*(y + NY*z), x fastest (utilities/indexing.cuh:10-13);
+ *   - populations are structure-of-arrays, f[i*Ncells + id]
+ *     (utilities/indexing.cuh:15-19), direction order of stencil_ct.cuh:9-16;
+ *   - fields are float32, radial sums float64, radial counts uint64
+ *     (utilities/types.cuh:6-11).
+ *
+ * Error behaviour: the reference prints and calls exit(1) on any CUDA error
+ * (utilities/cudaUtilities.cuh:9-19).  Every function here instead returns an
+ * mcg_status and never exits or traps; mcg_last_error_string() describes the
+ * last failure of the calling thread.
+ *
+ * Threading: one handle is driven by one host thread at a time.  Work is
+ * queued on the handle's stream (mcg_set_stream); functions that return host
+ * data synchronise that stream first.
+ */
+#ifndef MCG_H
+#define MCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCG_Q 27
+#define MCG_ABI_VERSION 1
+
+typedef enum mcg_status {
+    MCG_OK = 0,
+    MCG_ERR_INVALID_ARG = 1,  /* bad parameter, null pointer, size out of range */
+    MCG_ERR_OOM = 2,          /* device or host allocation failed */
+    MCG_ERR_CUDA = 3,         /* a CUDA runtime call or kernel launch failed */
+    MCG_ERR_NONFINITE = 4,    /* NaN/Inf detected by mcg_check_finite */
+    MCG_ERR_IO = 5,           /* file could not be created or fully written */
+    MCG_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    MCG_ERR_STATE = 7,        /* call not valid in the handle's current state */
+    MCG_ERR_UNSUPPORTED = 8,  /* option combination not implemented */
+    MCG_ERR_NO_DEVICE = 9     /* no CUDA device visible */
+} mcg_status;
+
+/* Population storage in HBM.  Arithmetic is float32 in both cases. */
+typedef enum mcg_storage {
+    MCG_STORAGE_F32 = 0,  /* reference precision (utilities/types.cuh:6-11) */
+    MCG_STORAGE_F16 = 1   /* offset by w_i*rho0, colour split as a fraction (extension) */
+} mcg_storage;
+
+/* What happens at the y ghost planes. */
+typedef enum mcg_boundary {
+    /* jet inlet at y=0 and convective outlet at y=NY-1
+     * (jet/boundary_conditions.cuh:17-85,163-233) - the shipped driver main.cu */
+    MCG_BOUNDARY_JET = 0,
+    /* no boundary kernels: y ghost-plane populations are never rewritten and the
+     * colour gradient reads the frozen ghost densities - what launch_bubble +
+     * launch_Macros + launch_collistream alone do in the reference */
+    MCG_BOUNDARY_CLOSED = 1,
+    /* x, y and z periodic both for streaming and for the colour gradient
+     * (extension: a true periodic box; the reference never wraps y) */
+    MCG_BOUNDARY_PERIODIC = 2
+} mcg_boundary;
+
+/*
+ * Case parameters.  Field names mirror constants.cuh:8-76 one-to-one so a
+ * constants.cuh can be generated from them (mcg_write_constants_header).
+ * mcg_params_default() fills the values shipped in constants.cuh;
+ * mcg_params_derive() recomputes nu, taur, taub and sigma from Re, We and the
+ * jet scales exactly as constants.cuh:59-76 does (float arithmetic).
+ */
+typedef struct mcg_params {
+    int32_t NX, NY, NZ;                 /* constants.cuh:14-16 */
+    int32_t NSTEP, NOUTPUT;             /* constants.cuh:8-9 */
+    int32_t NSTATS_START_STEP;          /* constants.cuh:10 */
+    int32_t write_vti_output;           /* constants.cuh:11 */
+    int32_t sponge_cells;               /* constants.cuh:17 */
+    float jet_radius, jet_x0, jet_z0, jet_velocity;              /* constants.cuh:32-35 */
+    float bubble_radius, bubble_x0, bubble_y0, bubble_z0;        /* constants.cuh:38-41 */
+    float rhor0, rhob0;                 /* constants.cuh:56-57 */
+    float Re, We;                       /* constants.cuh:59,71 */
+    float nu, taur, taub, sigma;        /* constants.cuh:60-64,73 */
+    float beta_recolor;                 /* constants.cuh:74 */
+    float sponge_K;                     /* utilities/mathUtilities.cuh:50 */
+    /* ---- options with no counterpart in constants.cuh ---- */
+    int32_t boundary;                   /* mcg_boundary */
+    int32_t storage;                    /* mcg_storage */
+    uint64_t seed;                      /* counter-based hash seed for all noise */
+    float init_noise;                   /* relative amplitude of uniform noise on initial populations */
+    float inlet_noise;                  /* relative amplitude of uniform noise on the inlet velocity */
+    int32_t bubble_red_inside;          /* 0: blue sphere in red (bubble/bubbleIn.cuh:20-22); 1: red in blue */
+    int32_t reserved[9];
+} mcg_params;
+
+typedef struct mcg_handle mcg_handle;
+
+/* ---------------- parameters ---------------- */
+
+/* Values of constants.cuh as shipped (128x400x128, Re 5000, We 2000, jet). */
+mcg_status mcg_params_default(mcg_params *p);
+/* nu = 2*R*U/Re, taur = taub = 0.5 + nu/cs2, sigma = rhob0*U^2*2R/We
+ * (constants.cuh:60-73); jet_x0/z0 and bubble centres = (N-1)/2 (:33-34,39-41). */
+mcg_status mcg_params_derive(mcg_params *p);
+/* Sets taur = taub = tau and nu = (tau - 0.5)*cs2 directly (bubble cases that
+ * are specified by tau and sigma rather than Re and We). */
+mcg_status mcg_params_set_tau(mcg_params *p, float tau);
+/* Writes a constants.cuh-compatible header (same names, same
+ * `name = static_cast<T>(value)` text form that post/case_config.py:30-35 and
+ * post/mean_profile_io.py:12-18 parse). */
+mcg_status mcg_write_constants_header(const mcg_params *p, const char *path);
+
+/* ---------------- lifetime (memory.cuh:58-133) ---------------- */
+
+/* allocate_device_memory() + allocate_mean_fields_device() equivalent.
+ * All device memory is owned by the handle and zero-filled like memory.cuh:79-95. */
+mcg_status mcg_create(const mcg_params *p, mcg_handle **out);
+/* free_device_memory() + free_mean_fields_runtime() equivalent. */
+mcg_status mcg_destroy(mcg_handle *h);
+/* cudaStream_t passed as void*; NULL selects the handle's own stream. */
+mcg_status mcg_set_stream(mcg_handle *h, void *stream);
+mcg_status mcg_synchronize(mcg_handle *h);
+mcg_status mcg_get_params(const mcg_handle *h, mcg_params *out);
+/* Bytes of device memory held by the handle. */
+mcg_status mcg_device_bytes(const mcg_handle *h, uint64_t *out);
+
+/* ---------------- initial conditions ---------------- */
+
+/* launch_jetDensity + launch_Injet (launch.cuh:19-29 -> kernels.cu:29-56,
+ * jet/jetIn.cuh:13-62): red at rest everywhere, blue disc on the y=0 plane. */
+mcg_status mcg_init_jet(mcg_handle *h);
+/* launch_bubble (launch.cuh:13-17 -> kernels.cu:13-27, bubble/bubbleIn.cuh:10-39). */
+mcg_status mcg_init_bubble(mcg_handle *h);
+
+/* ---------------- state transfer (host buffers, reference layout) ---------------- */
+
+/* Populations f(t) in reference layout fr[i*Ncells+id], fb[...] (float32, Q*Ncells each).
+ * set: every interior node's 27 populations plus the y-ghost-plane values that
+ *      interior nodes receive from the boundary (slots no kernel rewrites keep them).
+ * get: interior nodes as the reference's d.fir/d.fib hold them; ghost nodes are 0. */
+mcg_status mcg_set_populations(mcg_handle *h, const float *fr, const float *fb);
+mcg_status mcg_get_populations(mcg_handle *h, float *fr, float *fb);
+/* Macroscopic fields, Ncells each, as d.rhor..d.uz hold them (memory.cuh:11-25),
+ * ghost nodes included.  set_fields defines the ghost-node densities the colour
+ * gradient reads and the outlet state (any of the pointers may be NULL). */
+mcg_status mcg_set_fields(mcg_handle *h, const float *rhor, const float *rhob,
+                          const float *ux, const float *uy, const float *uz);
+mcg_status mcg_get_fields(mcg_handle *h, float *rhor, float *rhob,
+                          float *ux, float *uy, float *uz);
+/* Non-equilibrium stress Pixx,Pixy,Piyy,Piyz,Pizz,Pixz (6*Ncells, that order). */
+mcg_status mcg_get_stress(mcg_handle *h, float *pi6);
+
+/* ---------------- the per-step launch sequence (main.cu:52-104) ---------------- */
+
+/* launch_Macros (launch.cuh:31-37 -> kernels.cu:60-76, lbm.cuh:82-165). */
+mcg_status mcg_macros(mcg_handle *h);
+/* launch_accumulate_radial_moments (launch.cuh:75-90 -> kernels.cu:188-233). */
+mcg_status mcg_accumulate_radial_moments(mcg_handle *h);
+/* launch_collistream (launch.cuh:92-99 -> kernels.cu:78-94, lbm.cuh:184-293).
+ * Advances the step counter. */
+mcg_status mcg_collistream(mcg_handle *h);
+/* launch_inlet_bc (launch.cuh:101-108 -> kernels.cu:98-114,
+ * jet/boundary_conditions.cuh:17-85).  Uses the moments of the last mcg_macros. */
+mcg_status mcg_inlet_bc(mcg_handle *h);
+/* launch_neumann_bc (launch.cuh:110-118 -> kernels.cu:116-132,
+ * jet/boundary_conditions.cuh:163-233). */
+mcg_status mcg_neumann_bc(mcg_handle *h);
+
+/* nsteps iterations of main.cu:52-82 (macros, radial statistics once
+ * step >= NSTATS_START_STEP as update_radial_statistics_start does
+ * (meanF/meanFieldsRT.cuh:173-190), collision, inlet, outlet) through the fused
+ * B200 kernels.  Same results as the granular sequence above.  No host sync. */
+mcg_status mcg_step(mcg_handle *h, int32_t nsteps);
+/* Same, but times the nsteps on the handle's stream with CUDA events and
+ * returns the elapsed milliseconds (synchronises). */
+mcg_status mcg_step_timed(mcg_handle *h, int32_t nsteps, float *ms);
+/* Same steps with a CUDA event between consecutive launches: ms_total is the
+ * whole span, ms_kernels[0..2] the summed device time of the moments,
+ * boundary and collision launches (bench/roofline instrumentation). */
+mcg_status mcg_step_profiled(mcg_handle *h, int32_t nsteps, float *ms_total, float *ms_kernels);
+/* Current step counter (number of completed collisions). */
+mcg_status mcg_get_step(const mcg_handle *h, int64_t *step);
+/* Kernel launches issued by this handle since creation. */
+mcg_status mcg_launch_count(const mcg_handle *h, uint64_t *count);
+
+/* ---------------- mean fields and radial statistics (meanF/) ---------------- */
+
+/* Forces statistics on (1) or off (0) regardless of NSTATS_START_STEP;
+ * -1 restores the automatic start. */
+mcg_status mcg_set_radial_statistics(mcg_handle *h, int32_t mode);
+/* Device->host copies of the radial sums (meanF/meanFieldsRT.cuh:305-329):
+ * five float64 arrays and one uint64 array of NY*NR_BINS, r fastest.
+ * Any pointer may be NULL. */
+mcg_status mcg_get_radial(mcg_handle *h, double *sum_uy, double *sum_uy2,
+                          double *sum_ur, double *sum_ur2, double *sum_uruy,
+                          uint64_t *count);
+/* Radial-statistics state (meanF/memoryMeanFields.cuh:39-45). */
+mcg_status mcg_get_radial_state(const mcg_handle *h, int32_t *started,
+                                uint32_t *start_step, uint32_t *samples);
+/* launch_compute_total_tke + launch_update_tke_average (main.cu:73-90,
+ * kernels.cu:136-166): sum of 0.5|u|^2 over interior nodes (float64 on the
+ * device, returned as the reference's float32) and its running average. */
+mcg_status mcg_compute_tke(mcg_handle *h, int32_t step, float *tke_total, float *tke_avg);
+/* launch_update_uy_average (launch.cuh:63-73 -> kernels.cu:168-186) - defined
+ * but never launched by the reference; here it feeds mean_profiles/uy_avg.bin. */
+mcg_status mcg_update_uy_average(mcg_handle *h);
+mcg_status mcg_get_uy_average(mcg_handle *h, float *uy_avg, uint32_t *samples);
+
+/* ---------------- diagnostics ---------------- */
+
+/* Float64 sums over interior nodes of the current populations f(t):
+ * out[0]=sum fr, out[1]=sum fb, out[2..4]=sum (fr+fb) c.  */
+mcg_status mcg_conservation_sums(mcg_handle *h, double out[5]);
+/* Scans fields and populations; MCG_ERR_NONFINITE if any NaN/Inf. */
+mcg_status mcg_check_finite(mcg_handle *h);
+
+/* ---------------- output files (io/save_data.cuh, meanF/meanFieldsRT.cuh) ---------------- */
+
+/* initialize_mean_fields_runtime (meanF/meanFieldsRT.cuh:132-162): creates
+ * <root>/JET_VTK/Re<Re>_We<We>/{mean_profiles,vti_data}, opens tke_*.bin and
+ * writes case_info.txt. */
+mcg_status mcg_output_open(mcg_handle *h, const char *root_dir);
+/* The NOUTPUT block of main.cu:73-103 for `step`: tke sample (stdout line +
+ * tke_*.bin), radial outputs when statistics run, VTI when write_vti_output. */
+mcg_status mcg_output_step(mcg_handle *h, int32_t step);
+/* write_radial_profile_outputs (meanF/meanFieldsRT.cuh:297-336). */
+mcg_status mcg_write_radial_outputs(mcg_handle *h);
+/* write_vti (io/save_data.cuh:137-200) of the current fields to `path`. */
+mcg_status mcg_write_vti(mcg_handle *h, const char *path);
+/* mean_profiles/uy_avg.bin (float32, Ncells) read by post/binConversionVti.py:22-28. */
+mcg_status mcg_write_uy_average(mcg_handle *h);
+/* Paths chosen by mcg_output_open (empty strings before it). */
+mcg_status mcg_output_dirs(const mcg_handle *h, char *case_dir, char *mean_dir,
+                           char *vti_dir, size_t cap);
+mcg_status mcg_output_close(mcg_handle *h);
+
+/* ---------------- errors / introspection ---------------- */
+
+const char *mcg_last_error_string(void);
+const char *mcg_status_string(mcg_status s);
+int32_t mcg_abi_version(void);
+/* Number of CUDA devices (0 without a GPU; never fails). */
+int32_t mcg_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCG_H */

@@ -1,0 +1,64 @@
+// internal.hpp - the solver handle behind the C ABI (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/mcg.h"
+#include "kernels.cuh"
+
+struct mcg_handle {
+    mcg_params p{};
+    mcg::DeviceState s{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int cur = 0;            // pops[cur] holds f(t) in pull layout
+    int64_t step = 0;       // completed collisions
+    uint64_t launches = 0;  // kernels launched through this handle
+
+    // radial statistics (meanF/memoryMeanFields.cuh:39-45)
+    int stats_mode = -1;  // -1 automatic from NSTATS_START_STEP, 0 off, 1 on
+    bool stats_started = false;
+    uint32_t stats_start_step = 0;
+    uint32_t stats_samples = 0;
+    std::vector<uint64_t> ncols;  // interior (x,z) columns per radial bin
+
+    // total kinetic energy state (meanF/memoryMeanFields.cuh:24-37)
+    bool first_tke = true;
+    float tke_total = 0.f, tke_avg = 0.f, tke_avg_prev = 0.f, tke_delta = 0.f, tke_abs_delta = 0.f;
+    uint32_t uy_avg_samples = 0;
+
+    double *d_scalar = nullptr;  // 8 doubles of device scratch for reductions
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> prof_events;  // mcg_step_profiled
+
+    // output files (meanF/meanFieldsRT.cuh:23-33)
+    std::string case_dir, mean_dir, vti_dir;
+    FILE *f_tke_total = nullptr, *f_tke_avg = nullptr, *f_tke_diff = nullptr;
+};
+
+namespace mcg {
+
+// Records the error text for mcg_last_error_string() and returns s.
+mcg_status fail(mcg_status s, const std::string &msg);
+mcg_status cuda_fail(cudaError_t e, const char *what);
+
+// Radial count materialisation: samples * ncols[rb] on interior y rows.
+void radial_counts(const mcg_handle *h, uint64_t *count);
+
+// io.cpp
+mcg_status io_open(mcg_handle *h, const char *root);
+mcg_status io_close(mcg_handle *h);
+mcg_status io_write_case_metadata(mcg_handle *h);
+mcg_status io_write_radial(mcg_handle *h);
+mcg_status io_write_vti(mcg_handle *h, const std::string &path);
+mcg_status io_write_tke_sample(mcg_handle *h, int32_t step);
+mcg_status io_write_uy_average(mcg_handle *h);
+std::string base64_encode(const unsigned char *data, size_t len);
+
+}  // namespace mcg

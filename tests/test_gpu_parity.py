@@ -1,0 +1,206 @@
+"""Parity of the CUDA step with the CPU oracle and with the reference's own CUDA build.
+
+Tolerances (float32 arithmetic on both sides; the reference and this solver
+contract multiply-adds differently, so results agree to rounding, not bits):
+  populations after 100 steps from the same state:  max-abs <= 2e-5
+  macroscopic fields / stress:                       max-abs <= 2e-5
+  radial float64 sums:                               |d sum| <= 2e-5 * count per bin
+                                                     (the field tolerance per sample)
+Radial counts are integers and must match exactly.  The granular launch
+sequence and the fused step compute the boundary values in different kernels,
+whose multiply-add contraction may differ, so they agree to 1e-6, not bits.
+"""
+import numpy as np
+import pytest
+
+from helpers import initial_state, interior, maxabs, pops_interior, psi_of, run_reference
+from conftest import ref_binary
+from multicomponent_color_gradient_b200 import Solver, get_case
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+POP_ATOL = 2e-5
+FIELD_ATOL = 2e-5
+SAMPLE_ATOL = 2e-5
+
+SMALL = [("bubble_24_ref", 100, 10**9, 1e-6), ("jet_24x40x24", 100, 20, 1e-6), ("jet_32x48x32", 100, 20, 0.0)]
+
+
+def _solver_from_state(case, state):
+    fr, fb, fields = state
+    S = Solver(case)
+    S.set_fields(**fields)
+    S.set_populations(fr, fb)
+    return S
+
+
+def _oracle_from_state(case, state, precision):
+    fr, fb, fields = state
+    O = Oracle(case, precision)
+    O.set_fields(**fields)
+    O.set_populations(fr, fb)
+    return O
+
+
+def _radial_close(a, b, atol=SAMPLE_ATOL):
+    np.testing.assert_array_equal(a["count"], b["count"])
+    cnt = np.maximum(np.asarray(b["count"], np.float64), 1.0)
+    for k in ("sum_uy", "sum_uy2", "sum_ur", "sum_ur2", "sum_uruy"):
+        err = np.max(np.abs(a[k] - b[k]) / cnt)
+        assert err <= atol, (k, err)
+
+
+@pytest.mark.parametrize("name,steps,stats_from,noise", SMALL)
+@pytest.mark.parametrize("precision", [32, 64])
+def test_step_matches_oracle(name, steps, stats_from, noise, precision):
+    case = get_case(name, NSTATS_START_STEP=stats_from)
+    state = initial_state(case, noise=noise, seed=7)
+    S = _solver_from_state(case, state)
+    O = _oracle_from_state(case, state, precision)
+    S.step(steps)
+    O.step(steps)
+    assert S.current_step == O.current_step == steps
+    fr, fb = S.get_populations()
+    ofr, ofb = O.get_populations()
+    e_r = maxabs(pops_interior(fr, case), pops_interior(ofr, case))
+    e_b = maxabs(pops_interior(fb, case), pops_interior(ofb, case))
+    m = interior(case)
+    F, OF = S.get_fields(), O.get_fields()
+    errs = {k: maxabs(F[k][m], OF[k][m]) for k in ("rhor", "rhob", "ux", "uy", "uz")}
+    print(f"{name} fp{precision}: pops r {e_r:.3e} b {e_b:.3e} fields {errs}")
+    assert e_r <= POP_ATOL and e_b <= POP_ATOL, (e_r, e_b)
+    for k, e in errs.items():
+        assert e <= FIELD_ATOL, (k, e)
+    assert maxabs(S.get_stress().reshape(6, -1)[:, m], O.get_stress().reshape(6, -1)[:, m]) <= FIELD_ATOL
+    if case["boundary"] == "jet":
+        # outlet state on y = NY-1 (jet/boundary_conditions.cuh:184-196)
+        NX, NY, NZ = case["NX"], case["NY"], case["NZ"]
+        sel = np.zeros((NZ, NY, NX), bool)
+        sel[1:-1, NY - 1, 1:-1] = True
+        sel = sel.reshape(-1)
+        for k in ("rhor", "rhob", "ux", "uy", "uz"):
+            assert maxabs(F[k][sel], OF[k][sel]) <= FIELD_ATOL, ("outlet", k)
+        assert S.radial_state() == O.radial_state()
+        _radial_close(S.get_radial(), O.get_radial())
+
+
+@pytest.mark.parametrize("name,steps,stats_from,noise", SMALL)
+def test_granular_sequence_equals_fused_step(name, steps, stats_from, noise):
+    """launch_Macros/accumulate/collistream/inlet/neumann == the fused step."""
+    case = get_case(name, NSTATS_START_STEP=stats_from)
+    state = initial_state(case, noise=noise, seed=3)
+    A = _solver_from_state(case, state)
+    B = _solver_from_state(case, state)
+    A.step(steps)
+    for s in range(steps):
+        B.launch_Macros()
+        if s >= stats_from:
+            B.launch_accumulate_radial_moments()
+        B.launch_collistream()
+        if case["boundary"] == "jet":
+            B.launch_inlet_bc()
+            B.launch_neumann_bc()
+    fa, fb_ = A.get_populations()
+    ga, gb = B.get_populations()
+    assert maxabs(fa, ga) <= 1e-6 and maxabs(fb_, gb) <= 1e-6
+    Fa, Fb = A.get_fields(), B.get_fields()
+    for k in Fa:
+        assert maxabs(Fa[k], Fb[k]) <= 1e-6, k
+    if case["boundary"] == "jet":
+        _radial_close(A.get_radial(), B.get_radial(), atol=1e-6)
+        assert A.radial_state() == B.radial_state()
+
+
+@pytest.mark.parametrize("name", ["bubble_24_ref", "jet_24x40x24", "bubble_64"])
+def test_population_roundtrip(name):
+    case = get_case(name)
+    fr, fb, fields = initial_state(case, noise=1e-3, seed=11)
+    S = _solver_from_state(case, (fr, fb, fields))
+    gr, gb = S.get_populations()
+    np.testing.assert_array_equal(pops_interior(gr, case), pops_interior(fr, case))
+    np.testing.assert_array_equal(pops_interior(gb, case), pops_interior(fb, case))
+    # ghost nodes are reported as zero
+    assert not np.any(gr.reshape(27, -1)[:, ~interior(case)])
+
+
+@pytest.mark.parametrize("name,steps,stats_from", [("bubble_24_ref", 100, 10**9), ("jet_24x40x24", 100, 20),
+                                                   ("jet_32x48x32", 100, 20)])
+def test_matches_reference_build_small(name, steps, stats_from):
+    if ref_binary(name) is None:
+        pytest.skip("reference build oracle/_ref/ref_%s not present" % name)
+    case = get_case(name)
+    state = initial_state(case, noise=1e-6 if case["boundary"] != "jet" else 0.0, seed=5)
+    R = run_reference(name, case, steps, stats_from, state=state)
+    # the reference driver starts statistics at stats_from; so does NSTATS_START_STEP
+    S2 = Solver(get_case(name, NSTATS_START_STEP=stats_from))
+    S2.set_fields(**state[2])
+    S2.set_populations(state[0], state[1])
+    S2.step(steps)
+    fr, fb = S2.get_populations()
+    assert maxabs(pops_interior(fr, case), pops_interior(R["fr"], case)) <= POP_ATOL
+    assert maxabs(pops_interior(fb, case), pops_interior(R["fb"], case)) <= POP_ATOL
+    F = S2.get_fields()
+    m = interior(case)
+    for k in ("rhor", "rhob", "ux", "uy", "uz"):
+        assert maxabs(F[k][m], R[k][m]) <= FIELD_ATOL, k
+    if case["boundary"] == "jet":
+        _radial_close(S2.get_radial(), R)
+
+
+@pytest.mark.parametrize("name,stats_from", [("bubble_64_ref", 10**9), ("jet_128x256x128", 50)])
+def test_matches_reference_build_full_size(name, stats_from):
+    """BASELINE shapes, 100 steps from each code's own initial condition:
+    max-abs on populations and on psi (the north_star's parity measure)."""
+    if ref_binary(name) is None:
+        pytest.skip("reference build oracle/_ref/ref_%s not present" % name)
+    case = get_case(name, NSTATS_START_STEP=stats_from)
+    steps = 100
+    R = run_reference(name, case, steps, stats_from)
+    S = Solver(case)
+    if case["boundary"] == "jet":
+        S.init_jet()
+    else:
+        S.init_bubble()
+    S.step(steps)
+    fr, fb = S.get_populations()
+    e_r = maxabs(pops_interior(fr, case), pops_interior(R["fr"], case))
+    e_b = maxabs(pops_interior(fb, case), pops_interior(R["fb"], case))
+    F = S.get_fields()
+    m = interior(case)
+    e_psi = maxabs(psi_of(F["rhor"][m], F["rhob"][m]), psi_of(R["rhor"][m], R["rhob"][m]))
+    print(f"{name}: max|dfr|={e_r:.3e} max|dfb|={e_b:.3e} max|dpsi|={e_psi:.3e}")
+    assert e_r <= POP_ATOL and e_b <= POP_ATOL
+    assert e_psi <= 1e-4
+    if case["boundary"] == "jet":
+        _radial_close(S.get_radial(), R)
+
+
+def test_periodic_bubble_conserves_each_colour():
+    case = get_case("bubble_64", NSTEP=200)
+    S = Solver(case)
+    S.init_bubble()
+    s0 = S.conservation_sums()
+    S.step(200)
+    s1 = S.conservation_sums()
+    assert abs(s1[0] - s0[0]) / s0[0] < 2e-6
+    assert abs(s1[1] - s0[1]) / s0[1] < 2e-6
+    assert S.check_finite()
+
+
+def test_periodic_bubble_matches_oracle():
+    case = get_case("bubble_64")
+    S = Solver(case)
+    S.init_bubble()
+    fr, fb = S.get_populations()
+    F = S.get_fields()
+    O = Oracle(case, 64)
+    O.set_fields(F["rhor"], F["rhob"], F["ux"], F["uy"], F["uz"])
+    O.set_populations(fr, fb)
+    # the oracle's periodic ghost densities are refreshed from the interior
+    S.step(50)
+    O.step(50)
+    a, b = S.get_populations()
+    oa, ob = O.get_populations()
+    assert maxabs(pops_interior(a, case), pops_interior(oa, case)) <= POP_ATOL
+    assert maxabs(pops_interior(b, case), pops_interior(ob, case)) <= POP_ATOL
