@@ -88,6 +88,7 @@ SIGNATURES = {
     "mcg_get_uy_average": [_P, _F, _U32],
     "mcg_conservation_sums": [_P, _D],
     "mcg_check_finite": [_P],
+    "mcg_conservation_sums_static": [_P, _P, C.c_int32, C.c_int32, C.c_int32, _P, _P],
     "mcg_output_open": [_P, C.c_char_p],
     "mcg_output_step": [_P, C.c_int32],
     "mcg_write_radial_outputs": [_P],
