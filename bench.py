@@ -51,6 +51,19 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def traffic_per_launch(cells: int):
+    """DRAM bytes (read + write) of one k_fused launch scaled from the committed
+    ncu summary (profiles/k_fused_*.md, line `dram_bytes_per_node: <value>`), or None."""
+    import glob
+    import re
+
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "k_fused_*.md"))):
+        m = re.search(r"dram_bytes_per_node:\s*([0-9.]+)", open(path).read())
+        if m:
+            return int(float(m.group(1)) * cells)
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
 
@@ -209,6 +222,9 @@ def main():
     ap.add_argument("--no-f16", action="store_true", help="skip the float16-storage companion measurement")
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
+    ap.add_argument("--shape", default=None,
+                    help="NXxNYxNZ override of the case grid (smaller profiling captures); not a bench line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -226,7 +242,11 @@ def main():
     hbm_peak, peak_kind = load_peaks()
 
     def measure(storage: str):
-        case = get_case(args.case, storage=storage, NSTATS_START_STEP=0, seed=20260101 + rank, inlet_noise=0.01)
+        over = {}
+        if args.shape:
+            over = dict(zip(("NX", "NY", "NZ"), (int(v) for v in args.shape.lower().split("x"))))
+        case = get_case(args.case, storage=storage, NSTATS_START_STEP=0, seed=20260101 + rank, inlet_noise=0.01,
+                        **over)
         S = Solver(case)
         S.init_jet() if case["boundary"] == "jet" else S.init_bubble()
         S.step(args.warmup)
@@ -244,24 +264,23 @@ def main():
     case, S, ms, per_kernel, launches, clocks = measure(args.storage)
     cells = case["NX"] * case["NY"] * case["NZ"]
     mlups = world * cells * args.steps / (ms * 1e3)
-    pop_bytes = 216 if args.storage == "f32" else 108  # algorithmic bytes per node per pass
-    kernels = {}
-    for k in ("moments", "collide"):
-        t = per_kernel[k] / args.steps  # ms per launch
-        kernels[k] = {"ms_per_launch": round(t, 6), "GBps": round(pop_bytes * cells / (t * 1e-3) / 1e9, 1)}
-    kernels["boundary"] = {"ms_per_launch": round(per_kernel["boundary"] / args.steps, 6)}
-    dom = max(("moments", "collide"), key=lambda k: per_kernel[k])
-    ach = kernels[dom]["GBps"]
-    step_gbps = 2 * pop_bytes * cells / (ms / args.steps * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_" + dom, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "peak_kind": peak_kind,
-                "traffic": None, "algorithmic_bytes_per_node": pop_bytes,
+    step_bytes = 432 if args.storage == "f32" else 216  # algorithmic bytes per lattice update
+    t_fused = per_kernel["fused"] / args.steps  # ms per launch
+    t_bc = per_kernel["boundary"] / args.steps
+    ach = step_bytes * cells / (t_fused * 1e-3) / 1e9
+    step_gbps = step_bytes * cells / (ms / args.steps * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_fused", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(ach / hbm_peak, 4), "peak_kind": peak_kind, "traffic": traffic_per_launch(cells),
+                "algorithmic_bytes_per_node": step_bytes,
                 "step_achieved": round(step_gbps, 1), "step_frac": round(step_gbps / hbm_peak, 4),
-                "step_algorithmic_bytes_per_node": 2 * pop_bytes, "kernels": kernels}
+                "kernels": {"k_fused": {"ms_per_launch": round(t_fused, 6)},
+                            "k_boundary": {"ms_per_launch": round(t_bc, 6)}}}
 
     # end to end through the public API: host state in, K steps, fields out
     e2e = None
     try:
+        if args.no_e2e:
+            raise RuntimeError("skipped (--no-e2e)")
         fr_h = torch.empty(27 * cells, dtype=torch.float32, pin_memory=True)
         fb_h = torch.empty(27 * cells, dtype=torch.float32, pin_memory=True)
         fl_h = {k: torch.empty(cells, dtype=torch.float32, pin_memory=True) for k in ("rhor", "rhob", "ux", "uy", "uz")}
@@ -316,7 +335,7 @@ def main():
                    "tau": round(case["taub"], 6), "sigma": round(case["sigma"], 6), "beta": case["beta_recolor"],
                    "radial_statistics": "on", "inlet_noise": 0.01,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (pop_bytes * cells / 1e6)},
+                   "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (step_bytes / 2 * cells / 1e6)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
         "f16_store": f16,
     }

@@ -183,8 +183,9 @@ mcg_status mcg_step(mcg_handle *h, int32_t nsteps);
  * returns the elapsed milliseconds (synchronises). */
 mcg_status mcg_step_timed(mcg_handle *h, int32_t nsteps, float *ms);
 /* Same steps with a CUDA event between consecutive launches: ms_total is the
- * whole span, ms_kernels[0..2] the summed device time of the moments,
- * boundary and collision launches (bench/roofline instrumentation). */
+ * whole span, ms_kernels[0] the summed device time of the fused step kernel,
+ * ms_kernels[1] that of the boundary launch, ms_kernels[2] is 0
+ * (bench/roofline instrumentation; ms_kernels has room for 3). */
 mcg_status mcg_step_profiled(mcg_handle *h, int32_t nsteps, float *ms_total, float *ms_kernels);
 /* Current step counter (number of completed collisions). */
 mcg_status mcg_get_step(const mcg_handle *h, int64_t *step);

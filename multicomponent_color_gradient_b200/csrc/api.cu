@@ -61,6 +61,9 @@ using mcg::fail;
 
 namespace {
 
+// Shared memory of one fused-step CTA: three CTAs per SM (228 KB per SM).
+constexpr int kFusedSmemPerBlock = 75 * 1024;
+
 float derive_omega(const mcg_params &p) {
     // omega_sponge (mathUtilities.cuh:60-90) with K = 0: 1/(0.5 + nu/cs^2)
     return 1.0f / std::fma(p.nu, mcg::kInvCs2, 0.5f);
@@ -71,6 +74,7 @@ mcg_status validate(const mcg_params *p) {
     MCG_REQUIRE(p->NX >= 4 && p->NY >= 4 && p->NZ >= 4, "NX, NY, NZ must be >= 4 (ghost shell included)");
     const double n = double(p->NX) * p->NY * p->NZ;
     MCG_REQUIRE(n < 2147483647.0, "NX*NY*NZ must be < 2^31");
+    MCG_REQUIRE(p->NX <= 256, "NX must be <= 256 (one CTA row of the fused step spans the x extent)");
     MCG_REQUIRE(p->boundary >= 0 && p->boundary <= 2, "unknown boundary mode");
     MCG_REQUIRE(p->storage == MCG_STORAGE_F32 || p->storage == MCG_STORAGE_F16, "unknown storage");
     MCG_REQUIRE(std::isfinite(p->taub) && p->taub > 0.5f, "taub must be > 0.5");
@@ -136,7 +140,7 @@ size_t pop_buffer_bytes(const mcg_params &p) {
 void release(mcg_handle *h) {
     mcg::io_close(h);
     void *ptrs[] = {h->s.pops[0], h->s.pops[1], h->s.mom, h->s.psi[0], h->s.psi[1],
-                    h->s.radial,  h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar};
+                    h->s.radial,  h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar, h->s.bmom};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
@@ -179,17 +183,33 @@ bool stats_for_step(mcg_handle *h) {
     return h->stats_started;
 }
 
-mcg_status run_steps(mcg_handle *h, int32_t nsteps) {
+// One fused step (k_fused, then k_boundary for the jet).  The moment planes in
+// HBM are not written by the fused kernel; they are refreshed on demand.
+mcg_status one_fused_step(mcg_handle *h, bool *ran_boundary) {
     const bool jet = h->p.boundary == MCG_BOUNDARY_JET;
-    for (int32_t n = 0; n < nsteps; ++n) {
-        const bool stats = stats_for_step(h);
-        MCG_LAUNCH(h, mcg::launch_moments(h->s, h->cur, h->step, stats, h->stream), "moments kernel");
-        if (stats) ++h->stats_samples;
-        if (jet) MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, h->stream), "boundary kernel");
-        MCG_LAUNCH(h, mcg::launch_collide(h->s, h->cur, h->step, h->stream), "collision kernel");
-        h->cur ^= 1;
-        ++h->step;
-    }
+    const bool stats = stats_for_step(h);
+    MCG_LAUNCH(h, mcg::launch_fused(h->s, h->tiling, h->cur, h->step, stats, h->stream), "fused step kernel");
+    if (stats) ++h->stats_samples;
+    if (jet) MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, true, h->stream), "boundary kernel");
+    if (ran_boundary) *ran_boundary = jet;
+    h->cur ^= 1;
+    ++h->step;
+    h->mom_stale = true;
+    return MCG_OK;
+}
+
+mcg_status run_steps(mcg_handle *h, int32_t nsteps) {
+    for (int32_t n = 0; n < nsteps; ++n)
+        if (mcg_status s = one_fused_step(h, nullptr)) return s;
+    return MCG_OK;
+}
+
+// Moment planes of the last completed step (what the reference's d.rhor ..
+// d.Pixz hold after it): recomputed from that step's input buffer.
+mcg_status ensure_moments(mcg_handle *h) {
+    if (!h->mom_stale || h->step == 0) return MCG_OK;
+    MCG_LAUNCH(h, mcg::launch_moments(h->s, h->cur ^ 1, h->step - 1, false, h->stream), "moments kernel");
+    h->mom_stale = false;
     return MCG_OK;
 }
 
@@ -285,6 +305,7 @@ mcg_status mcg_create(const mcg_params *p, mcg_handle **out) {
     g.sz = p->NX * p->NY;
     g.boundary = p->boundary;
     g.storage = p->storage;
+    g.slots = p->storage == MCG_STORAGE_F16 ? mcg::kQ : 2 * mcg::kQ;
     fill_physics(h);
     compute_ncols(h);
     const size_t N = g.N;
@@ -297,6 +318,9 @@ mcg_status mcg_create(const mcg_params *p, mcg_handle **out) {
     if (e == cudaSuccess) e = alloc_zero(&h->s.psi[0], N * 4);
     if (e == cudaSuccess) e = alloc_zero(&h->s.psi[1], N * 4);
     if (e == cudaSuccess) e = alloc_zero(&h->s.radial, 5 * M * 8);
+    if (e == cudaSuccess) e = alloc_zero(&h->s.bmom, size_t(2) * p->NZ * mcg::kMomCount * p->NX * 4);
+    h->tiling = mcg::fused_tiling(g, kFusedSmemPerBlock);
+    if (e == cudaSuccess) e = mcg::fused_configure(h->tiling.smem_bytes);
     if (e == cudaSuccess) e = alloc_zero(&h->s.uy_avg, N * 4);
     h->s.partials_cap = mcg::conservation_blocks(g);
     if (e == cudaSuccess) e = alloc_zero(&h->s.partials, size_t(h->s.partials_cap) * 5 * 8);
@@ -374,8 +398,9 @@ static mcg_status init_common(mcg_handle *h, int mode) {
     if (mcg_status s = reset_counters(h)) return s;
     const mcg_params &p = h->p;
     MCG_LAUNCH(h, mcg::launch_init_fields(h->s, mode, p.bubble_red_inside, p.bubble_radius * p.bubble_radius,
-                                          p.bubble_x0, p.bubble_y0, p.bubble_z0, 0.f, h->stream),
+                                          p.bubble_x0, p.bubble_y0, p.bubble_z0, h->stream),
                "init fields");
+    h->mom_stale = false;
     MCG_LAUNCH(h, mcg::launch_refresh_psi(h->s, h->stream), "init psi");
     MCG_LAUNCH(h, mcg::launch_init_pops(h->s, mode, nullptr, nullptr, p.init_noise, h->stream), "init populations");
     return MCG_OK;
@@ -442,11 +467,13 @@ mcg_status mcg_set_fields(mcg_handle *h, const float *rhor, const float *rhob, c
                      "upload field");
     MCG_LAUNCH(h, mcg::launch_refresh_psi(h->s, h->stream), "refresh psi");
     MCG_CUDA(cudaStreamSynchronize(h->stream), "set fields");
+    h->mom_stale = false;
     return MCG_OK;
 }
 
 mcg_status mcg_get_fields(mcg_handle *h, float *rhor, float *rhob, float *ux, float *uy, float *uz) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = ensure_moments(h)) return s;
     const size_t N = h->s.g.N;
     float *dst[5] = {rhor, rhob, ux, uy, uz};
     for (int k = 0; k < 5; ++k)
@@ -460,6 +487,7 @@ mcg_status mcg_get_fields(mcg_handle *h, float *rhor, float *rhob, float *ux, fl
 mcg_status mcg_get_stress(mcg_handle *h, float *pi6) {
     if (mcg_status s = check_handle(h)) return s;
     MCG_REQUIRE(pi6 != nullptr, "pi6 is null");
+    if (mcg_status s = ensure_moments(h)) return s;
     const size_t N = h->s.g.N;
     MCG_CUDA(cudaMemcpyAsync(pi6, h->s.mom + size_t(mcg::kMomPXX) * N, 6 * N * 4, cudaMemcpyDeviceToHost, h->stream),
              "download stress");
@@ -472,6 +500,7 @@ mcg_status mcg_get_stress(mcg_handle *h, float *pi6) {
 mcg_status mcg_macros(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
     MCG_LAUNCH(h, mcg::launch_moments(h->s, h->cur, h->step, false, h->stream), "moments kernel");
+    h->mom_stale = false;
     return MCG_OK;
 }
 
@@ -498,14 +527,14 @@ mcg_status mcg_collistream(mcg_handle *h) {
 mcg_status mcg_inlet_bc(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
     if (h->step == 0) return fail(MCG_ERR_STATE, "mcg_inlet_bc needs a preceding mcg_collistream");
-    MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur, h->step - 1, 0, h->stream), "inlet kernel");
+    MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur, h->step - 1, 0, false, h->stream), "inlet kernel");
     return MCG_OK;
 }
 
 mcg_status mcg_neumann_bc(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
     if (h->step == 0) return fail(MCG_ERR_STATE, "mcg_neumann_bc needs a preceding mcg_collistream");
-    MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur, h->step - 1, 1, h->stream), "outlet kernel");
+    MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur, h->step - 1, 1, false, h->stream), "outlet kernel");
     return MCG_OK;
 }
 
@@ -530,33 +559,31 @@ mcg_status mcg_step_profiled(mcg_handle *h, int32_t nsteps, float *ms_total, flo
     if (mcg_status s = check_handle(h)) return s;
     MCG_REQUIRE(nsteps >= 0 && ms_total != nullptr && ms_kernels != nullptr, "bad arguments");
     const bool jet = h->p.boundary == MCG_BOUNDARY_JET;
-    const size_t need = size_t(nsteps) * 3 + 1;
+    const size_t need = size_t(nsteps) * 2 + 1;
     while (h->prof_events.size() < need) {
         cudaEvent_t e;
         MCG_CUDA(cudaEventCreate(&e), "event create");
         h->prof_events.push_back(e);
     }
-    // kind of the launch that ends at event k+1: 0 moments, 1 boundary, 2 collision
+    // kind of the launch that ends at event k+1: 0 fused step, 1 boundary
     std::vector<int> kind;
     kind.reserve(need);
     size_t ev = 0;
     MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
     for (int32_t n = 0; n < nsteps; ++n) {
         const bool stats = stats_for_step(h);
-        MCG_LAUNCH(h, mcg::launch_moments(h->s, h->cur, h->step, stats, h->stream), "moments kernel");
+        MCG_LAUNCH(h, mcg::launch_fused(h->s, h->tiling, h->cur, h->step, stats, h->stream), "fused step kernel");
         if (stats) ++h->stats_samples;
         MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
         kind.push_back(0);
         if (jet) {
-            MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, h->stream), "boundary kernel");
+            MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, true, h->stream), "boundary kernel");
             MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
             kind.push_back(1);
         }
-        MCG_LAUNCH(h, mcg::launch_collide(h->s, h->cur, h->step, h->stream), "collision kernel");
-        MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
-        kind.push_back(2);
         h->cur ^= 1;
         ++h->step;
+        h->mom_stale = true;
     }
     MCG_CUDA(cudaEventSynchronize(h->prof_events[ev - 1]), "event synchronize");
     ms_kernels[0] = ms_kernels[1] = ms_kernels[2] = 0.0f;
@@ -616,6 +643,7 @@ mcg_status mcg_get_radial_state(const mcg_handle *h, int32_t *started, uint32_t 
 
 mcg_status mcg_compute_tke(mcg_handle *h, int32_t step, float *tke_total, float *tke_avg) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = ensure_moments(h)) return s;
     MCG_LAUNCH(h, mcg::launch_tke(h->s, h->d_scalar, h->stream), "tke kernel");
     double tot = 0;
     MCG_CUDA(cudaMemcpyAsync(&tot, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download tke");
@@ -632,6 +660,7 @@ mcg_status mcg_compute_tke(mcg_handle *h, int32_t step, float *tke_total, float 
 
 mcg_status mcg_update_uy_average(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = ensure_moments(h)) return s;
     MCG_LAUNCH(h, mcg::launch_uy_average(h->s, h->uy_avg_samples, h->stream), "uy average kernel");
     ++h->uy_avg_samples;
     return MCG_OK;
@@ -663,6 +692,7 @@ mcg_status mcg_conservation_sums(mcg_handle *h, double out[5]) {
 
 mcg_status mcg_check_finite(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = ensure_moments(h)) return s;
     MCG_LAUNCH(h, mcg::launch_check_finite(h->s, h->cur, h->s.flag, h->stream), "finite check kernel");
     int flag = 0;
     MCG_CUDA(cudaMemcpyAsync(&flag, h->s.flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "download flag");
@@ -709,6 +739,7 @@ mcg_status mcg_write_radial_outputs(mcg_handle *h) {
 mcg_status mcg_write_vti(mcg_handle *h, const char *path) {
     if (mcg_status s = check_handle(h)) return s;
     MCG_REQUIRE(path != nullptr, "path is null");
+    if (mcg_status s = ensure_moments(h)) return s;
     return mcg::io_write_vti(h, path);
 }
 

@@ -20,6 +20,8 @@ struct mcg_handle {
     int cur = 0;            // pops[cur] holds f(t) in pull layout
     int64_t step = 0;       // completed collisions
     uint64_t launches = 0;  // kernels launched through this handle
+    mcg::FusedTiling tiling{};
+    bool mom_stale = false;  // moment planes lag the last fused step
 
     // radial statistics (meanF/memoryMeanFields.cuh:39-45)
     int stats_mode = -1;  // -1 automatic from NSTATS_START_STEP, 0 off, 1 on

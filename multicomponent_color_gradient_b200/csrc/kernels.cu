@@ -1,25 +1,35 @@
 // kernels.cu - the D3Q27 colour-gradient step on B200 (sm_100a).
 //
-// One step is two HBM passes over the lattice plus a plane-sized launch:
-//   k_moments  pulls f(t) from pops[cur] (27+27 coalesced loads per node),
-//              forms rho_r, rho_b, u, Pi^neq (lbm.cuh:82-165) and psi, and in
-//              the same pass accumulates the radial statistics
-//              (kernels.cu:188-233) with warp segmented reductions instead of
-//              six global atomics per node.
+// The step is one HBM pass (k_fused) plus a plane-sized launch (k_boundary):
+//   k_fused    a CTA owns a tile of rows (y) and marches a chunk of z planes.
+//              For each plane it pulls f(t) for its rows plus a one-row halo
+//              from the population buffer (row-blocked layout, so a pulled row
+//              is nine contiguous segments), forms rho_r, rho_b, u, Pi^neq
+//              (lbm.cuh:82-165) and psi into shared memory, accumulates the
+//              radial statistics (kernels.cu:188-233) with warp segmented
+//              reductions, and then relaxes the previous plane
+//              (lbm.cuh:184-293): Hermite-regularised BGK, colour-gradient
+//              perturbation and recolouring, with the gradient taken from the
+//              same step's psi in shared memory (the reference needs a kernel
+//              boundary for this), storing the post-collision values at each
+//              node (pull layout, coalesced rows).  Moments never go to HBM.
 //   k_boundary the inlet (jet/boundary_conditions.cuh:17-85) and convective
 //              outlet (jet/boundary_conditions.cuh:163-233) of the same step,
-//              one thread per boundary column; the values land in the y ghost
-//              planes of pops[cur^1].
-//   k_collide  relaxes every node (lbm.cuh:184-293): Hermite-regularised BGK,
-//              colour-gradient perturbation and recolouring, with the
-//              gradient from the 26 neighbouring psi values, and stores the
-//              54 post-collision values at the node itself in pops[cur^1]
-//              (fully coalesced stores; the next k_moments pulls them).
+//              one thread per boundary column, from the fluid-plane moments
+//              k_fused leaves in bmom; values land in the y ghost planes of
+//              the new buffer.
+// The granular launch sequence of the reference (k_moments, k_collide,
+// k_boundary, k_accumulate_radial) is kept for callers that drive the
+// launchers one by one; it writes the moment planes to HBM like the reference.
 // The reference's in-place push buffer becomes a ping-pong pull pair; the
 // populations a reference step never rewrites (y=1 slots fed by non-jet
-// inlet columns, y=NY-2 slots fed by ghost columns) are the ghost-plane
-// values of both buffers that no kernel writes, so results are the same.
+// inlet columns, y=NY-2 slots fed by ghost columns) are ghost-plane values of
+// both buffers that no kernel writes, so results are the same.
+#include <cooperative_groups.h>
 #include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cstdlib>
 
 #include "kernels.cuh"
 #include "lattice.cuh"
@@ -27,36 +37,38 @@
 namespace mcg {
 namespace {
 
+namespace cg = cooperative_groups;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------ storage codecs
 
 struct CodecF32 {
+    static constexpr int kGroupSlots = 6;
     const float *__restrict__ rd;
     float *__restrict__ wr;
-    uint32_t N;
+    int NX;
+    // pull: `grow` = offset of the source row's group segment
     template <int I>
-    __device__ __forceinline__ void load(uint32_t s, float &r, float &b) const {
-        r = __ldg(rd + size_t(I) * N + s);
-        b = __ldg(rd + size_t(kQ + I) * N + s);
+    __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
+        r = __ldg(rd + grow + size_t(0 * 3 + dir_cx(I) + 1) * NX + xs);
+        b = __ldg(rd + grow + size_t(1 * 3 + dir_cx(I) + 1) * NX + xs);
     }
     template <int I>
-    __device__ __forceinline__ void store(uint32_t id, float r, float b) const {
-        wr[size_t(I) * N + id] = r;
-        wr[size_t(kQ + I) * N + id] = b;
+    __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
+        wr[row + size_t(slot_f32(I, 0)) * NX + x] = r;
+        wr[row + size_t(slot_f32(I, 1)) * NX + x] = b;
     }
-    // Write into a buffer other than wr (initialisation).
-    __device__ __forceinline__ static void store_to(void *buf, uint32_t N, int i, uint32_t id, float r, float b,
-                                                    float) {
+    __device__ __forceinline__ static void store_to(void *buf, const Geometry &g, int i, int x, int y, int z, float r,
+                                                    float b, float) {
         float *p = static_cast<float *>(buf);
-        p[size_t(i) * N + id] = r;
-        p[size_t(kQ + i) * N + id] = b;
+        p[pop_index(g, slot_f32(i, 0), x, y, z)] = r;
+        p[pop_index(g, slot_f32(i, 1), x, y, z)] = b;
     }
-    __device__ __forceinline__ static void load_from(const void *buf, uint32_t N, int i, uint32_t s, float &r,
-                                                     float &b, float) {
+    __device__ __forceinline__ static void load_from(const void *buf, const Geometry &g, int i, int x, int y, int z,
+                                                     float &r, float &b, float) {
         const float *p = static_cast<const float *>(buf);
-        r = p[size_t(i) * N + s];
-        b = p[size_t(kQ + i) * N + s];
+        r = p[pop_index(g, slot_f32(i, 0), x, y, z)];
+        b = p[pop_index(g, slot_f32(i, 1), x, y, z)];
     }
 };
 
@@ -82,26 +94,27 @@ __device__ __forceinline__ void f16_decode(__half2 h, float w, float rho0, float
 }
 
 struct CodecF16 {
+    static constexpr int kGroupSlots = 3;
     const __half2 *__restrict__ rd;
     __half2 *__restrict__ wr;
-    uint32_t N;
+    int NX;
     float rho0;
     template <int I>
-    __device__ __forceinline__ void load(uint32_t s, float &r, float &b) const {
-        const __half2 h = __ldg(rd + size_t(I) * N + s);
+    __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
+        const __half2 h = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
         f16_decode(h, Dir<I>::w, rho0, r, b);
     }
     template <int I>
-    __device__ __forceinline__ void store(uint32_t id, float r, float b) const {
-        wr[size_t(I) * N + id] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
+    __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
+        wr[row + size_t(slot_f16(I)) * NX + x] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
     }
-    __device__ __forceinline__ static void store_to(void *buf, uint32_t N, int i, uint32_t id, float r, float b,
-                                                    float rho0) {
-        static_cast<__half2 *>(buf)[size_t(i) * N + id] = f16_encode(r, b, 1.0f / dir_w(i), rho0);
+    __device__ __forceinline__ static void store_to(void *buf, const Geometry &g, int i, int x, int y, int z, float r,
+                                                    float b, float rho0) {
+        static_cast<__half2 *>(buf)[pop_index(g, slot_f16(i), x, y, z)] = f16_encode(r, b, 1.0f / dir_w(i), rho0);
     }
-    __device__ __forceinline__ static void load_from(const void *buf, uint32_t N, int i, uint32_t s, float &r,
-                                                     float &b, float rho0) {
-        f16_decode(static_cast<const __half2 *>(buf)[size_t(i) * N + s], dir_w(i), rho0, r, b);
+    __device__ __forceinline__ static void load_from(const void *buf, const Geometry &g, int i, int x, int y, int z,
+                                                     float &r, float &b, float rho0) {
+        f16_decode(static_cast<const __half2 *>(buf)[pop_index(g, slot_f16(i), x, y, z)], dir_w(i), rho0, r, b);
     }
 };
 
@@ -109,11 +122,11 @@ template <class C>
 __host__ __device__ C make_codec(const DeviceState &s, int cur);
 template <>
 __host__ __device__ CodecF32 make_codec<CodecF32>(const DeviceState &s, int cur) {
-    return CodecF32{static_cast<const float *>(s.pops[cur]), static_cast<float *>(s.pops[cur ^ 1]), s.g.N};
+    return CodecF32{static_cast<const float *>(s.pops[cur]), static_cast<float *>(s.pops[cur ^ 1]), s.g.NX};
 }
 template <>
 __host__ __device__ CodecF16 make_codec<CodecF16>(const DeviceState &s, int cur) {
-    return CodecF16{static_cast<const __half2 *>(s.pops[cur]), static_cast<__half2 *>(s.pops[cur ^ 1]), s.g.N,
+    return CodecF16{static_cast<const __half2 *>(s.pops[cur]), static_cast<__half2 *>(s.pops[cur ^ 1]), s.g.NX,
                     s.ph.f16_rho0};
 }
 
@@ -142,65 +155,478 @@ __device__ __forceinline__ float inlet_velocity(const Physics &ph, int64_t step,
     return ph.jet_velocity * (1.0f + (2.0f * u - 1.0f) * ph.inlet_noise);
 }
 
-// Pull source of direction I for interior node (x,y,z) with id.
-//  x and z are periodic over the interior through the ghost shell (the push
-//  side wraps with bounds.cuh:23-60); y sources on a ghost plane are the
-//  boundary's slots and are not wrapped (boundary writes are unwrapped,
-//  boundary_conditions.cuh:73,137); in the periodic box y wraps too.
+__host__ __device__ __forceinline__ int wrap_interior(int v, int n) { return v == 0 ? n - 2 : (v == n - 1 ? 1 : v); }
+
+// Pull sources of interior node (x,y,z).  x and z are periodic over the
+// interior through the ghost shell (the push side wraps with
+// bounds.cuh:23-60); y sources on a ghost plane are the boundary's slots and
+// are not wrapped laterally (boundary writes are unwrapped,
+// boundary_conditions.cuh:73,137); in the periodic box y wraps too.
+template <class C>
 struct PullMap {
-    int wxp, wxm, wzp, wzm, wyp, wym;
+    long long own_row;              // offset of row (y,z)
+    long long step_y, step_z;       // row offsets of y+1, z+1
+    long long wzp, wzm, wyp, wym;   // wrap corrections (row offsets)
+    int wxp, wxm;                   // wrap corrections (x)
+    int NX;
     bool gy_p, gy_m;
     __device__ __forceinline__ PullMap(const Geometry &g, int x, int y, int z, bool periodic) {
+        NX = g.NX;
+        own_row = (long long)pop_row(g, y, z);
+        step_y = (long long)g.slots * g.NX;
+        step_z = step_y * g.NY;
         wxp = (x == 1) ? (g.NX - 2) : 0;
         wxm = (x == g.NX - 2) ? -(g.NX - 2) : 0;
-        wzp = (z == 1) ? g.sz * (g.NZ - 2) : 0;
-        wzm = (z == g.NZ - 2) ? -g.sz * (g.NZ - 2) : 0;
-        wyp = (periodic && y == 1) ? g.sy * (g.NY - 2) : 0;
-        wym = (periodic && y == g.NY - 2) ? -g.sy * (g.NY - 2) : 0;
+        wzp = (z == 1) ? step_z * (g.NZ - 2) : 0;
+        wzm = (z == g.NZ - 2) ? -step_z * (g.NZ - 2) : 0;
+        wyp = (periodic && y == 1) ? step_y * (g.NY - 2) : 0;
+        wym = (periodic && y == g.NY - 2) ? -step_y * (g.NY - 2) : 0;
         gy_p = !periodic && y == 1;
         gy_m = !periodic && y == g.NY - 2;
     }
+    // offset of the group segment of direction I's source row, and source x
     template <int I>
-    __device__ __forceinline__ uint32_t src(const Geometry &g, uint32_t id) const {
+    __device__ __forceinline__ void src(int x, size_t &grow, int &xs) const {
         using D = Dir<I>;
-        int s = int(id) - (D::cx + g.sy * D::cy + g.sz * D::cz);
+        const long long o = own_row - D::cy * step_y - D::cz * step_z;
         bool ghost = false;
         if constexpr (D::cy == 1) ghost = gy_p;
         if constexpr (D::cy == -1) ghost = gy_m;
-        int corr = 0;
-        if constexpr (D::cx == 1) corr += wxp;
-        if constexpr (D::cx == -1) corr += wxm;
-        if constexpr (D::cz == 1) corr += wzp;
-        if constexpr (D::cz == -1) corr += wzm;
-        if (ghost) corr = 0;
-        if constexpr (D::cy == 1) corr += wyp;
-        if constexpr (D::cy == -1) corr += wym;
-        return uint32_t(s + corr);
+        int xc = 0;
+        long long oc = 0;
+        if constexpr (D::cx == 1) xc = wxp;
+        if constexpr (D::cx == -1) xc = wxm;
+        if constexpr (D::cz == 1) oc = wzp;
+        if constexpr (D::cz == -1) oc = wzm;
+        if (ghost) {
+            xc = 0;
+            oc = 0;
+        }
+        if constexpr (D::cy == 1) oc += wyp;
+        if constexpr (D::cy == -1) oc += wym;
+        grow = size_t(o + oc) + size_t(dir_group(I) * C::kGroupSlots) * size_t(NX);
+        xs = x - D::cx + xc;
     }
 };
 
-// Same map for a runtime direction (init/gather kernels).
-__device__ __forceinline__ uint32_t pull_src_rt(const Geometry &g, int x, int y, int z, int i) {
+// Runtime-direction pull source (init/gather/diagnostic kernels): source
+// coordinates of direction i for interior node (x,y,z).
+__device__ __forceinline__ void pull_src_rt(const Geometry &g, int x, int y, int z, int i, int &xs, int &ys, int &zs) {
     const bool periodic = g.boundary == kBoundaryPeriodic;
-    int xs = x - dir_cx(i), ys = y - dir_cy(i), zs = z - dir_cz(i);
+    xs = x - dir_cx(i);
+    ys = y - dir_cy(i);
+    zs = z - dir_cz(i);
     const bool ghost_plane = !periodic && (ys == 0 || ys == g.NY - 1);
     if (!ghost_plane) {
-        if (xs == 0) xs = g.NX - 2;
-        else if (xs == g.NX - 1) xs = 1;
-        if (zs == 0) zs = g.NZ - 2;
-        else if (zs == g.NZ - 1) zs = 1;
+        xs = wrap_interior(xs, g.NX);
+        zs = wrap_interior(zs, g.NZ);
     }
-    if (periodic) {
-        if (ys == 0) ys = g.NY - 2;
-        else if (ys == g.NY - 1) ys = 1;
-    }
-    return uint32_t(xs) + uint32_t(g.sy) * uint32_t(ys) + uint32_t(g.sz) * uint32_t(zs);
+    if (periodic) ys = wrap_interior(ys, g.NY);
 }
 
-// Runtime-direction tables in constant memory for the non-hot kernels.
 __constant__ int c_cx[kQ] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
 __constant__ int c_cy[kQ] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
 __constant__ int c_cz[kQ] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+
+// ------------------------------------------------------------------ per-node pieces
+
+// Pull the 54 populations of interior node (x,y,z) and form its moments
+// (lbm.cuh:106-164, same summation order).
+template <class C, bool kPeriodic>
+__device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &codec, int x, int y, int z) {
+    const PullMap<C> pm(g, x, y, z, kPeriodic);
+    float sumr = 0.f, sumb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    float Axx = 0.f, Axy = 0.f, Ayy = 0.f, Ayz = 0.f, Azz = 0.f, Axz = 0.f;
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        using D = Dir<i>;
+        size_t grow;
+        int xs;
+        pm.template src<i>(x, grow, xs);
+        float fr, fb;
+        codec.template load<i>(grow, xs, fr, fb);
+        sumr += fr;
+        sumb += fb;
+        const float gi = fr + fb;
+        if constexpr (D::cx == 1) jx += gi;
+        if constexpr (D::cx == -1) jx -= gi;
+        if constexpr (D::cy == 1) jy += gi;
+        if constexpr (D::cy == -1) jy -= gi;
+        if constexpr (D::cz == 1) jz += gi;
+        if constexpr (D::cz == -1) jz -= gi;
+        Axx += gi * D::Hxx;
+        if constexpr (D::Hxy != 0.0f) Axy += gi * D::Hxy;
+        Ayy += gi * D::Hyy;
+        if constexpr (D::Hyz != 0.0f) Ayz += gi * D::Hyz;
+        Azz += gi * D::Hzz;
+        if constexpr (D::Hxz != 0.0f) Axz += gi * D::Hxz;
+    });
+    NodeMoments m;
+    const float rho = sumr + sumb;
+    const float inv = 1.0f / rho;
+    m.rr = sumr;
+    m.rb = sumb;
+    m.ux = jx * inv;
+    m.uy = jy * inv;
+    m.uz = jz * inv;
+    m.pxx = Axx - rho * m.ux * m.ux;
+    m.pxy = Axy - rho * m.ux * m.uy;
+    m.pyy = Ayy - rho * m.uy * m.uy;
+    m.pyz = Ayz - rho * m.uy * m.uz;
+    m.pzz = Azz - rho * m.uz * m.uz;
+    m.pxz = Axz - rho * m.ux * m.uz;
+    return m;
+}
+
+// Relax one node and store its 54 post-collision values (lbm.cuh:184-293).
+// Opposite directions are evaluated together: equilibrium and regularised
+// non-equilibrium split into even and odd parts, the perturbation Omega2 is
+// even (cos^2) and the recolouring Delta odd (cos phi).  psi_at(cx,cy,cz)
+// returns the neighbour's psi, read unwrapped like forces.cuh:31 (ghost psi
+// is what the reference sees there).
+template <class C, class PsiAt>
+__device__ __forceinline__ void collide_node(const Geometry &g, const Physics &ph, const C &codec, size_t row, int x,
+                                             int y, int z, const NodeMoments &m, PsiAt &&psi_at) {
+    const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
+    const EqTerms e = make_eq(m.ux, m.uy, m.uz);
+    const float rr = m.rr, rb = m.rb;
+    const float rT = rr + rb;
+    const float invrT = 1.0f / rT;
+    const float aR = rr * invrT, aB = rb * invrT;
+    const float oms = 1.0f - omega_at(ph, y);
+    const float Iind = 4.0f * rr * rb * invrT * invrT;
+    if (Iind <= 1e-4f) {  // bulk (lbm.cuh:216-247)
+        {
+            const float g0 = feq<0>(rT, e) + oms * fneq<0>(n);
+            codec.template store<0>(row, x, aR * g0, aB * g0);
+        }
+        static_for<(kQ - 1) / 2>([&](auto P) {
+            constexpr int i = 2 * decltype(P)::value + 1;
+            float ei, eo, ni, no;
+            feq_pair<i>(rT, e, ei, eo);
+            fneq_pair<i>(n, ni, no);
+            const float gi = ei + oms * ni, go = eo + oms * no;
+            codec.template store<i>(row, x, aR * gi, aB * gi);
+            codec.template store<i + 1>(row, x, aR * go, aB * go);
+        });
+        return;
+    }
+    // interface (lbm.cuh:249-292): colour gradient over the 26 neighbours
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    static_for<kQ - 1>([&](auto I) {
+        constexpr int i = decltype(I)::value + 1;
+        using D = Dir<i>;
+        const float wp = D::w * psi_at(D::cx, D::cy, D::cz);
+        if constexpr (D::cx == 1) sx += wp;
+        if constexpr (D::cx == -1) sx -= wp;
+        if constexpr (D::cy == 1) sy += wp;
+        if constexpr (D::cy == -1) sy -= wp;
+        if constexpr (D::cz == 1) sz += wp;
+        if constexpr (D::cz == -1) sz -= wp;
+    });
+    InterfaceTerms t;
+    t.Fx = kInvCs2 * sx;
+    t.Fy = kInvCs2 * sy;
+    t.Fz = kInvCs2 * sz;
+    t.absF = sqrtf(t.Fx * t.Fx + t.Fy * t.Fy + t.Fz * t.Fz);
+    t.has_dir = !(t.absF <= 1.0e-4f);
+    t.inv_absF = 1.0f / t.absF;
+    t.inv_absF2 = 1.0f / (t.absF * t.absF);
+    t.Ah_absF = ph.Ah * t.absF;
+    t.coeff_rho = ph.beta * ((rr * rb) / (rT * rT)) * rT;
+    {
+        const float g0 = feq<0>(rT, e) + oms * fneq<0>(n) + omega2<0>(t);
+        codec.template store<0>(row, x, aR * g0, aB * g0);
+    }
+    static_for<(kQ - 1) / 2>([&](auto P) {
+        constexpr int i = 2 * decltype(P)::value + 1;
+        float ei, eo, ni, no;
+        feq_pair<i>(rT, e, ei, eo);
+        fneq_pair<i>(n, ni, no);
+        const float o2 = omega2<i>(t);  // even: the same for i and its opposite
+        const float gi = ei + oms * ni + o2, go = eo + oms * no + o2;
+        const float d = recolour<i>(t);  // odd: -d for the opposite
+        codec.template store<i>(row, x, aR * gi + d, aB * gi - d);
+        codec.template store<i + 1>(row, x, aR * go - d, aB * go + d);
+    });
+}
+
+// ------------------------------------------------------------------ radial statistics
+
+// Warp-collective: one warp = 32 consecutive x at fixed (y,z).  Lanes with the
+// same radial bin form contiguous runs once split by the side of the jet axis
+// (the bin is monotone in |x - x0| on each side), so a segmented scan leaves
+// each run's sums in its last lane, which issues one float64 atomic per sum.
+// Counts are not accumulated per node: every sample adds the fixed number of
+// interior columns of a bin, so they are materialised on read.
+__device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int x, int y, int z, bool active,
+                                                       float ux, float uy, float uz) {
+    const Physics &ph = s.ph;
+    const int lane = threadIdx.x & 31;
+    unsigned key = 0xffffffffu;
+    double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0;
+    if (active) {
+        const float dx = float(x) - ph.jet_x0, dz = float(z) - ph.jet_z0;
+        const float r = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)));
+        const unsigned rb = unsigned(r);
+        if (rb < unsigned(ph.NRB)) {
+            key = (rb << 1) | (dx < 0.0f ? 1u : 0u);
+            float ur = 0.0f;
+            if (r > 1.0e-12f) ur = (ux * dx + uz * dz) / r;
+            const double duy = double(uy), dur = double(ur);
+            v0 = duy;
+            v1 = duy * duy;
+            v2 = dur;
+            v3 = dur * dur;
+            v4 = dur * duy;
+        }
+    }
+    if (__all_sync(kFull, key == 0xffffffffu)) return;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned ok = __shfl_up_sync(kFull, key, d);
+        const double o0 = __shfl_up_sync(kFull, v0, d);
+        const double o1 = __shfl_up_sync(kFull, v1, d);
+        const double o2 = __shfl_up_sync(kFull, v2, d);
+        const double o3 = __shfl_up_sync(kFull, v3, d);
+        const double o4 = __shfl_up_sync(kFull, v4, d);
+        if (lane >= d && ok == key) {
+            v0 += o0; v1 += o1; v2 += o2; v3 += o3; v4 += o4;
+        }
+    }
+    const unsigned next = __shfl_down_sync(kFull, key, 1);
+    const bool tail = (lane == 31) || (next != key);
+    if (tail && key != 0xffffffffu) {
+        const size_t M = size_t(s.g.NY) * ph.NRB;
+        const size_t mi = size_t(y) * ph.NRB + (key >> 1);
+        atomicAdd(s.radial + mi, v0);
+        atomicAdd(s.radial + M + mi, v1);
+        atomicAdd(s.radial + 2 * M + mi, v2);
+        atomicAdd(s.radial + 3 * M + mi, v3);
+        atomicAdd(s.radial + 4 * M + mi, v4);
+    }
+}
+
+// ------------------------------------------------------------------ the fused step
+
+constexpr int kFusedThreads = 256;
+#ifndef MCG_FUSED_MIN_BLOCKS
+#define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
+#endif
+
+template <class C, bool kStats, bool kPeriodic>
+__global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(const DeviceState s, const FusedTiling T, int cur,
+                                                            int64_t step) {
+    extern __shared__ float sm[];
+    const Geometry &g = s.g;
+    const int tpr = T.tpr;
+    const int rpt = kFusedThreads / tpr;
+    // row group of this thread; groups beyond rpt (when tpr does not divide
+    // the block) start past every row and only take part in the barriers
+    const int lr0 = threadIdx.x / tpr;
+    const int lr = lr0 < rpt ? lr0 : T.ty + 2;
+    const int x = threadIdx.x - lr0 * tpr;
+    const int y0 = 1 + int(blockIdx.x) * T.ty;
+    const int ty = min(T.ty, g.NY - 1 - y0);
+    const int z0 = 1 + int(blockIdx.y) * T.lz;
+    const int lz = min(T.lz, g.NZ - 1 - z0);
+    const int pstride = (T.ty + 2) * tpr;  // one psi plane of the ring
+    float *ring = sm;                      // [3][ty+2][tpr]
+    float *msm = sm + 3 * pstride;         // [2][ty][11][tpr]
+    const int mplane = T.ty * kMomCount * tpr;
+    const C codec = make_codec<C>(s, cur);
+    const float *__restrict__ psi_g = s.psi[step & 1];
+    const bool xin = x >= 1 && x <= g.NX - 2;
+    // Cluster of consecutive y-tiles (same z-chunk): a tile takes its halo
+    // rows from its neighbours' shared memory instead of pulling them.  Every
+    // CTA of a cluster runs the same number of planes, so the cluster
+    // barriers below are reached the same number of times by all of them.
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = T.cluster > 1 ? int(cluster.block_rank()) : 0;
+    const bool lower_nbr = T.cluster > 1 && crank > 0;
+    const bool upper_nbr = T.cluster > 1 && crank < T.cluster - 1;
+    const float *nbr_lo = lower_nbr ? cluster.map_shared_rank(ring, crank - 1) : nullptr;
+    const float *nbr_hi = upper_nbr ? cluster.map_shared_rank(ring, crank + 1) : nullptr;
+
+    for (int zp = z0 - 1; zp <= z0 + lz; ++zp) {
+        float *ringp = ring + (zp % 3) * pstride;
+        float *msmp = msm + (zp & 1) * mplane;
+        const bool own_plane = zp >= z0 && zp < z0 + lz;
+        // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
+        for (int r = lr; r < ty + 2; r += rpt) {
+            if ((r == 0 && lower_nbr) || (r == ty + 1 && upper_nbr)) continue;  // from a neighbour below
+            const int y = y0 - 1 + r;
+            const bool own_row = own_plane && r >= 1 && r <= ty;
+            NodeMoments m{};
+            bool have = false;
+            if (x < g.NX) {
+                int xn = x, yn = y, zn = zp;
+                bool pull;
+                if constexpr (kPeriodic) {
+                    xn = wrap_interior(x, g.NX);
+                    yn = wrap_interior(y, g.NY);
+                    zn = wrap_interior(zp, g.NZ);
+                    pull = true;
+                } else {
+                    pull = xin && y >= 1 && y <= g.NY - 2 && zp >= 1 && zp <= g.NZ - 2;
+                }
+                float ps;
+                if (pull) {
+                    m = pull_moments<C, kPeriodic>(g, codec, xn, yn, zn);
+                    have = true;
+                    ps = psi_of(m.rr, m.rb);
+                } else {
+                    ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
+                }
+                ringp[r * tpr + x] = ps;
+                if (own_row && xin) {
+                    float *q = msmp + (r - 1) * kMomCount * tpr + x;
+                    q[kMomRR * tpr] = m.rr;
+                    q[kMomRB * tpr] = m.rb;
+                    q[kMomUX * tpr] = m.ux;
+                    q[kMomUY * tpr] = m.uy;
+                    q[kMomUZ * tpr] = m.uz;
+                    q[kMomPXX * tpr] = m.pxx;
+                    q[kMomPXY * tpr] = m.pxy;
+                    q[kMomPYY * tpr] = m.pyy;
+                    q[kMomPYZ * tpr] = m.pyz;
+                    q[kMomPZZ * tpr] = m.pzz;
+                    q[kMomPXZ * tpr] = m.pxz;
+                    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
+                        // fluid-plane moments for the boundary launch
+                        float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
+                        const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy,
+                                                    m.pyz, m.pzz, m.pxz};
+#pragma unroll
+                        for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
+                    }
+                }
+            }
+            if constexpr (kStats) {
+                if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
+            }
+        }
+        if (T.cluster > 1) {
+            // own rows of plane zp are now visible cluster-wide; copy the
+            // neighbours' edge rows into this tile's halo rows.  A neighbour
+            // rewrites this ring slot only three planes later, after two more
+            // cluster barriers that this CTA has not reached yet.
+            cluster.sync();
+            const int off = (zp % 3) * pstride;
+            for (int i = threadIdx.x; i < g.NX; i += kFusedThreads) {
+                if (lower_nbr) ringp[i] = nbr_lo[off + T.ty * tpr + i];
+                if (upper_nbr) ringp[(ty + 1) * tpr + i] = nbr_hi[off + tpr + i];
+            }
+        }
+        __syncthreads();
+        // ---- relax plane zp-1 with psi of planes zp-2 .. zp
+        const int zc = zp - 1;
+        if (zc >= z0 && zc < z0 + lz) {
+            const float *pm = ring + ((zc + 2) % 3) * pstride;  // plane zc-1
+            const float *p0 = ring + (zc % 3) * pstride;        // plane zc
+            const float *pp = ring + ((zc + 1) % 3) * pstride;  // plane zc+1
+            const float *mc = msm + (zc & 1) * mplane;
+            for (int r = 1 + lr; r <= ty; r += rpt) {
+                if (!xin) continue;
+                const int y = y0 - 1 + r;
+                const float *q = mc + (r - 1) * kMomCount * tpr + x;
+                NodeMoments m;
+                m.rr = q[kMomRR * tpr];
+                m.rb = q[kMomRB * tpr];
+                m.ux = q[kMomUX * tpr];
+                m.uy = q[kMomUY * tpr];
+                m.uz = q[kMomUZ * tpr];
+                m.pxx = q[kMomPXX * tpr];
+                m.pxy = q[kMomPXY * tpr];
+                m.pyy = q[kMomPYY * tpr];
+                m.pyz = q[kMomPYZ * tpr];
+                m.pzz = q[kMomPZZ * tpr];
+                m.pxz = q[kMomPXZ * tpr];
+                const int base = r * tpr + x;
+                auto psi_at = [&](int cx, int cy, int cz) {
+                    const float *pl = cz < 0 ? pm : (cz > 0 ? pp : p0);
+                    return pl[base + cy * tpr + cx];
+                };
+                collide_node(g, s.ph, codec, pop_row(g, y, zc), x, y, zc, m, psi_at);
+            }
+        }
+        __syncthreads();
+    }
+    // no CTA leaves while a neighbour may still read its shared memory
+    if (T.cluster > 1) cluster.sync();
+}
+
+// ------------------------------------------------------------------ granular sequence
+
+constexpr int kBX = 32, kBY = 8;
+
+// launch_Macros equivalent: moments and psi of every interior node to HBM.
+template <class C, bool kPeriodic>
+__global__ void __launch_bounds__(kBX * kBY) k_moments(const DeviceState s, const C codec, int64_t step) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
+    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+    const NodeMoments m = pull_moments<C, kPeriodic>(g, codec, x, y, z);
+    const size_t N = g.N;
+    float *mom = s.mom;
+    mom[kMomRR * N + id] = m.rr;
+    mom[kMomRB * N + id] = m.rb;
+    mom[kMomUX * N + id] = m.ux;
+    mom[kMomUY * N + id] = m.uy;
+    mom[kMomUZ * N + id] = m.uz;
+    mom[kMomPXX * N + id] = m.pxx;
+    mom[kMomPXY * N + id] = m.pxy;
+    mom[kMomPYY * N + id] = m.pyy;
+    mom[kMomPYZ * N + id] = m.pyz;
+    mom[kMomPZZ * N + id] = m.pzz;
+    mom[kMomPXZ * N + id] = m.pxz;
+    const float ps = psi_of(m.rr, m.rb);
+    float *psi = s.psi[step & 1];
+    psi[id] = ps;
+    if constexpr (kPeriodic) {
+        // ghost mirrors so the unwrapped gradient stencil sees a periodic field
+        const int xs[2] = {x, x == 1 ? g.NX - 1 : (x == g.NX - 2 ? 0 : -1)};
+        const int ys[2] = {y, y == 1 ? g.NY - 1 : (y == g.NY - 2 ? 0 : -1)};
+        const int zs[2] = {z, z == 1 ? g.NZ - 1 : (z == g.NZ - 2 ? 0 : -1)};
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            const int xx = xs[k & 1], yy = ys[(k >> 1) & 1], zz = zs[(k >> 2) & 1];
+            if (xx >= 0 && yy >= 0 && zz >= 0)
+                psi[uint32_t(xx) + uint32_t(g.sy) * uint32_t(yy) + uint32_t(g.sz) * uint32_t(zz)] = ps;
+        }
+    }
+}
+
+// launch_collistream equivalent: relax from the moment planes and psi in HBM.
+template <class C>
+__global__ void __launch_bounds__(kBX * kBY, 4) k_collide(const DeviceState s, const C codec, int64_t step) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
+    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+    const size_t N = g.N;
+    const float *__restrict__ mom = s.mom;
+    NodeMoments m;
+    m.rr = __ldg(mom + kMomRR * N + id);
+    m.rb = __ldg(mom + kMomRB * N + id);
+    m.ux = __ldg(mom + kMomUX * N + id);
+    m.uy = __ldg(mom + kMomUY * N + id);
+    m.uz = __ldg(mom + kMomUZ * N + id);
+    m.pxx = __ldg(mom + kMomPXX * N + id);
+    m.pxy = __ldg(mom + kMomPXY * N + id);
+    m.pyy = __ldg(mom + kMomPYY * N + id);
+    m.pyz = __ldg(mom + kMomPYZ * N + id);
+    m.pzz = __ldg(mom + kMomPZZ * N + id);
+    m.pxz = __ldg(mom + kMomPXZ * N + id);
+    const float *__restrict__ psi = s.psi[step & 1];
+    auto psi_at = [&](int cx, int cy, int cz) { return __ldg(psi + (int(id) + cx + g.sy * cy + g.sz * cz)); };
+    collide_node(g, s.ph, codec, pop_row(g, y, z), x, y, z, m, psi_at);
+}
 
 // ------------------------------------------------------------------ boundary pieces
 
@@ -209,8 +635,8 @@ __constant__ int c_cz[kQ] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1,
 // are stored in the ghost plane y=0 of `dst` at (x,0,z), where the y=1 nodes
 // (x+cx, 1, z+cz) pull them.  `m` are the moments of fluid node (x,1,z).
 template <class C>
-__device__ __forceinline__ void inlet_column(const DeviceState &s, const C &codec_dst_only, void *dst, float *psi_dst,
-                                             int x, int z, int64_t step, const NodeMoments &m) {
+__device__ __forceinline__ void inlet_column(const DeviceState &s, void *dst, float *psi_dst, int x, int z,
+                                             int64_t step, const NodeMoments &m) {
     const Geometry &g = s.g;
     const Physics &ph = s.ph;
     const uint32_t idB = uint32_t(x) + uint32_t(g.sz) * uint32_t(z);
@@ -226,12 +652,11 @@ __device__ __forceinline__ void inlet_column(const DeviceState &s, const C &code
     const float oms = 1.0f - ph.omega_b;
     const EqTerms e = make_eq(0.0f, inlet_velocity(ph, step, x, z), 0.0f);
     const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
-    (void)codec_dst_only;
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         if constexpr (Dir<i>::cy == 1) {
             const float gi = feq<i>(rT, e) + oms * fneq<i>(n);
-            C::store_to(dst, g.N, i, idB, aR * gi, aB * gi, ph.f16_rho0);
+            C::store_to(dst, g, i, x, 0, z, aR * gi, aB * gi, ph.f16_rho0);
         }
     });
 }
@@ -270,245 +695,42 @@ __device__ __forceinline__ void outlet_column(const DeviceState &s, void *dst, f
         constexpr int i = decltype(I)::value;
         if constexpr (Dir<i>::cy == -1) {
             const float gi = feq<i>(rhoT, e) + oms * fneq<i>(n);
-            C::store_to(dst, g.N, i, idB, aR * gi, aB * gi, ph.f16_rho0);
+            C::store_to(dst, g, i, x, g.NY - 1, z, aR * gi, aB * gi, ph.f16_rho0);
         }
     });
 }
 
-// ------------------------------------------------------------------ radial statistics
-
-// Warp-collective: one warp = 32 consecutive x at fixed (y,z).  Lanes with the
-// same radial bin form contiguous runs once split by the side of the jet axis
-// (the bin is monotone in |x - x0| on each side), so a segmented scan leaves
-// each run's sums in its last lane, which issues one float64 atomic per sum.
-// Counts are not accumulated per node: every sample adds the fixed number of
-// interior columns of a bin, so they are materialised on read.
-__device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int x, int y, int z, bool active,
-                                                       float ux, float uy, float uz) {
-    const Physics &ph = s.ph;
-    const int lane = threadIdx.x & 31;
-    unsigned key = 0xffffffffu;
-    double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0;
-    if (active) {
-        const float dx = float(x) - ph.jet_x0, dz = float(z) - ph.jet_z0;
-        const float r = sqrtf(dx * dx + dz * dz);
-        const unsigned rb = unsigned(r);
-        if (rb < unsigned(ph.NRB)) {
-            key = (rb << 1) | (dx < 0.0f ? 1u : 0u);
-            float ur = 0.0f;
-            if (r > 1.0e-12f) ur = (ux * dx + uz * dz) / r;
-            const double duy = double(uy), dur = double(ur);
-            v0 = duy;
-            v1 = duy * duy;
-            v2 = dur;
-            v3 = dur * dur;
-            v4 = dur * duy;
-        }
-    }
-    if (__all_sync(kFull, key == 0xffffffffu)) return;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const unsigned ok = __shfl_up_sync(kFull, key, d);
-        const double o0 = __shfl_up_sync(kFull, v0, d);
-        const double o1 = __shfl_up_sync(kFull, v1, d);
-        const double o2 = __shfl_up_sync(kFull, v2, d);
-        const double o3 = __shfl_up_sync(kFull, v3, d);
-        const double o4 = __shfl_up_sync(kFull, v4, d);
-        if (lane >= d && ok == key) {
-            v0 += o0; v1 += o1; v2 += o2; v3 += o3; v4 += o4;
-        }
-    }
-    const unsigned next = __shfl_down_sync(kFull, key, 1);
-    const bool tail = (lane == 31) || (next != key);
-    if (tail && key != 0xffffffffu) {
-        const size_t M = size_t(s.g.NY) * ph.NRB;
-        const size_t m = size_t(y) * ph.NRB + (key >> 1);
-        atomicAdd(s.radial + m, v0);
-        atomicAdd(s.radial + M + m, v1);
-        atomicAdd(s.radial + 2 * M + m, v2);
-        atomicAdd(s.radial + 3 * M + m, v3);
-        atomicAdd(s.radial + 4 * M + m, v4);
-    }
-}
-
-// ------------------------------------------------------------------ the two step kernels
-
-constexpr int kBX = 32, kBY = 8;
-
-template <class C, bool kStats, bool kPeriodic>
-__global__ void __launch_bounds__(kBX * kBY) k_moments(const DeviceState s, const C codec, int64_t step) {
-    const Geometry &g = s.g;
-    const int x = blockIdx.x * kBX + threadIdx.x;
-    const int y = blockIdx.y * kBY + threadIdx.y;
-    const int z = blockIdx.z;
-    const bool active = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
-    NodeMoments m{};
-    if (active) {
-        const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
-        const PullMap pm(g, x, y, z, kPeriodic);
-        float sumr = 0.f, sumb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-        float Axx = 0.f, Axy = 0.f, Ayy = 0.f, Ayz = 0.f, Azz = 0.f, Axz = 0.f;
-        static_for<kQ>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            using D = Dir<i>;
-            float fr, fb;
-            codec.template load<i>(pm.template src<i>(g, id), fr, fb);
-            sumr += fr;
-            sumb += fb;
-            const float gi = fr + fb;
-            if constexpr (D::cx == 1) jx += gi;
-            if constexpr (D::cx == -1) jx -= gi;
-            if constexpr (D::cy == 1) jy += gi;
-            if constexpr (D::cy == -1) jy -= gi;
-            if constexpr (D::cz == 1) jz += gi;
-            if constexpr (D::cz == -1) jz -= gi;
-            Axx += gi * D::Hxx;
-            if constexpr (D::Hxy != 0.0f) Axy += gi * D::Hxy;
-            Ayy += gi * D::Hyy;
-            if constexpr (D::Hyz != 0.0f) Ayz += gi * D::Hyz;
-            Azz += gi * D::Hzz;
-            if constexpr (D::Hxz != 0.0f) Axz += gi * D::Hxz;
-        });
-        const float rho = sumr + sumb;
-        const float inv = 1.0f / rho;
-        m.rr = sumr;
-        m.rb = sumb;
-        m.ux = jx * inv;
-        m.uy = jy * inv;
-        m.uz = jz * inv;
-        m.pxx = Axx - rho * m.ux * m.ux;
-        m.pxy = Axy - rho * m.ux * m.uy;
-        m.pyy = Ayy - rho * m.uy * m.uy;
-        m.pyz = Ayz - rho * m.uy * m.uz;
-        m.pzz = Azz - rho * m.uz * m.uz;
-        m.pxz = Axz - rho * m.ux * m.uz;
-        const size_t N = g.N;
-        float *mom = s.mom;
-        mom[kMomRR * N + id] = m.rr;
-        mom[kMomRB * N + id] = m.rb;
-        mom[kMomUX * N + id] = m.ux;
-        mom[kMomUY * N + id] = m.uy;
-        mom[kMomUZ * N + id] = m.uz;
-        mom[kMomPXX * N + id] = m.pxx;
-        mom[kMomPXY * N + id] = m.pxy;
-        mom[kMomPYY * N + id] = m.pyy;
-        mom[kMomPYZ * N + id] = m.pyz;
-        mom[kMomPZZ * N + id] = m.pzz;
-        mom[kMomPXZ * N + id] = m.pxz;
-        const float ps = psi_of(sumr, sumb);
-        float *psi = s.psi[step & 1];
-        psi[id] = ps;
-        if constexpr (kPeriodic) {
-            // ghost mirrors so the unwrapped gradient stencil sees a periodic field
-            const int xs[2] = {x, x == 1 ? g.NX - 1 : (x == g.NX - 2 ? 0 : -1)};
-            const int ys[2] = {y, y == 1 ? g.NY - 1 : (y == g.NY - 2 ? 0 : -1)};
-            const int zs[2] = {z, z == 1 ? g.NZ - 1 : (z == g.NZ - 2 ? 0 : -1)};
-#pragma unroll
-            for (int k = 1; k < 8; ++k) {
-                const int xx = xs[k & 1], yy = ys[(k >> 1) & 1], zz = zs[(k >> 2) & 1];
-                if (xx >= 0 && yy >= 0 && zz >= 0)
-                    psi[uint32_t(xx) + uint32_t(g.sy) * uint32_t(yy) + uint32_t(g.sz) * uint32_t(zz)] = ps;
-            }
-        }
-    }
-    if constexpr (kStats) radial_accumulate_warp(s, x, y, z, active, m.ux, m.uy, m.uz);
-}
-
-template <class C>
-__global__ void __launch_bounds__(kBX * kBY, 4) k_collide(const DeviceState s, const C codec, int64_t step) {
-    const Geometry &g = s.g;
-    const Physics &ph = s.ph;
-    const int x = blockIdx.x * kBX + threadIdx.x;
-    const int y = blockIdx.y * kBY + threadIdx.y;
-    const int z = blockIdx.z;
-    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
-    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
-    const size_t N = g.N;
-    const float *__restrict__ mom = s.mom;
-    const float rr = __ldg(mom + kMomRR * N + id), rb = __ldg(mom + kMomRB * N + id);
-    const float vx = __ldg(mom + kMomUX * N + id), vy = __ldg(mom + kMomUY * N + id), vz = __ldg(mom + kMomUZ * N + id);
-    const NeqTerms n = make_neq(__ldg(mom + kMomPXX * N + id), __ldg(mom + kMomPXY * N + id),
-                                __ldg(mom + kMomPYY * N + id), __ldg(mom + kMomPYZ * N + id),
-                                __ldg(mom + kMomPZZ * N + id), __ldg(mom + kMomPXZ * N + id), vx, vy, vz);
-    const EqTerms e = make_eq(vx, vy, vz);
-    const float rT = rr + rb;
-    const float invrT = 1.0f / rT;
-    const float aR = rr * invrT, aB = rb * invrT;
-    const float oms = 1.0f - omega_at(ph, y);
-    const float Iind = 4.0f * rr * rb * invrT * invrT;
-    if (Iind <= 1e-4f) {  // bulk (lbm.cuh:216-247)
-        static_for<kQ>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            const float gi = feq<i>(rT, e) + oms * fneq<i>(n);
-            codec.template store<i>(id, aR * gi, aB * gi);
-        });
-        return;
-    }
-    // interface (lbm.cuh:249-292): colour gradient over the 26 neighbours,
-    // read unwrapped like forces.cuh:31 (ghost psi is what the reference sees)
-    const float *__restrict__ psi = s.psi[step & 1];
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    static_for<kQ - 1>([&](auto I) {
-        constexpr int i = decltype(I)::value + 1;
-        using D = Dir<i>;
-        const float p = __ldg(psi + (int(id) + D::cx + g.sy * D::cy + g.sz * D::cz));
-        const float wp = D::w * p;
-        if constexpr (D::cx == 1) sx += wp;
-        if constexpr (D::cx == -1) sx -= wp;
-        if constexpr (D::cy == 1) sy += wp;
-        if constexpr (D::cy == -1) sy -= wp;
-        if constexpr (D::cz == 1) sz += wp;
-        if constexpr (D::cz == -1) sz -= wp;
-    });
-    InterfaceTerms t;
-    t.Fx = kInvCs2 * sx;
-    t.Fy = kInvCs2 * sy;
-    t.Fz = kInvCs2 * sz;
-    t.absF = sqrtf(t.Fx * t.Fx + t.Fy * t.Fy + t.Fz * t.Fz);
-    t.has_dir = !(t.absF <= 1.0e-4f);
-    t.inv_absF = 1.0f / t.absF;
-    t.inv_absF2 = 1.0f / (t.absF * t.absF);
-    t.Ah_absF = ph.Ah * t.absF;
-    t.coeff_rho = ph.beta * ((rr * rb) / (rT * rT)) * rT;
-    static_for<kQ>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        const float gi = feq<i>(rT, e) + oms * fneq<i>(n) + omega2<i>(t);
-        const float d = recolour<i>(t);
-        codec.template store<i>(id, aR * gi + d, aB * gi - d);
-    });
-}
-
-__device__ __forceinline__ NodeMoments load_moments(const DeviceState &s, uint32_t id) {
-    const size_t N = s.g.N;
-    const float *m = s.mom;
+__device__ __forceinline__ NodeMoments load_moments(const float *m, size_t stride, size_t id) {
     NodeMoments r;
-    r.rr = m[kMomRR * N + id]; r.rb = m[kMomRB * N + id];
-    r.ux = m[kMomUX * N + id]; r.uy = m[kMomUY * N + id]; r.uz = m[kMomUZ * N + id];
-    r.pxx = m[kMomPXX * N + id]; r.pxy = m[kMomPXY * N + id]; r.pyy = m[kMomPYY * N + id];
-    r.pyz = m[kMomPYZ * N + id]; r.pzz = m[kMomPZZ * N + id]; r.pxz = m[kMomPXZ * N + id];
+    r.rr = m[kMomRR * stride + id]; r.rb = m[kMomRB * stride + id];
+    r.ux = m[kMomUX * stride + id]; r.uy = m[kMomUY * stride + id]; r.uz = m[kMomUZ * stride + id];
+    r.pxx = m[kMomPXX * stride + id]; r.pxy = m[kMomPXY * stride + id]; r.pyy = m[kMomPYY * stride + id];
+    r.pyz = m[kMomPYZ * stride + id]; r.pzz = m[kMomPZZ * stride + id]; r.pxz = m[kMomPXZ * stride + id];
     return r;
 }
 
-// Jet boundary of step `step` from its moments: blockIdx.z == 0 is the inlet
-// (y=0 plane), 1 the outlet (y=NY-1 plane).  Values go to the ghost planes of
-// buffer `wbuf` (the one the collision of this step writes) and to the psi
-// buffer of the next step; they run in their own small launch so the rarely
-// taken boundary code does not inflate the bulk kernels' register budget.
+// Jet boundary of step `step`: blockIdx.z == 0 is the inlet (y=0 plane), 1 the
+// outlet (y=NY-1 plane), unless `which` selects one.  Values go to the ghost
+// planes of buffer `wbuf` (the one the collision of this step writes) and to
+// the psi buffer of the next step.
 template <class C>
-__global__ void __launch_bounds__(256) k_boundary(const DeviceState s, int wbuf, int64_t step, int which) {
+__global__ void __launch_bounds__(256) k_boundary(const DeviceState s, int wbuf, int64_t step, int which,
+                                                  int from_bmom) {
     const Geometry &g = s.g;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.y * blockDim.y + threadIdx.y;
     if (x < 1 || x > g.NX - 2 || z < 1 || z > g.NZ - 2) return;
     const int side = which >= 0 ? which : int(blockIdx.z);
     float *psi_next = s.psi[(step + 1) & 1];
-    if (side == 0) {
-        const uint32_t idF = uint32_t(x) + uint32_t(g.sy) + uint32_t(g.sz) * uint32_t(z);
-        inlet_column<C>(s, C{}, s.pops[wbuf], psi_next, x, z, step, load_moments(s, idF));
+    NodeMoments m;
+    if (from_bmom) {
+        m = load_moments(s.bmom + (size_t(side) * g.NZ + z) * kMomCount * g.NX, size_t(g.NX), size_t(x));
     } else {
-        const uint32_t idF = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 2) + uint32_t(g.sz) * uint32_t(z);
-        outlet_column<C>(s, s.pops[wbuf], psi_next, x, z, load_moments(s, idF));
+        const int yF = side == 0 ? 1 : g.NY - 2;
+        m = load_moments(s.mom, size_t(g.N), size_t(x) + size_t(g.sy) * size_t(yF) + size_t(g.sz) * size_t(z));
     }
+    if (side == 0) inlet_column<C>(s, s.pops[wbuf], psi_next, x, z, step, m);
+    else outlet_column<C>(s, s.pops[wbuf], psi_next, x, z, m);
 }
 
 __global__ void __launch_bounds__(kBX * kBY) k_accumulate_radial(const DeviceState s) {
@@ -550,9 +772,9 @@ __global__ void k_init_fields(const DeviceState s, int mode, int red_inside, flo
     } else {
         int xx = x, yy = y, zz = z;
         if (g.boundary == kBoundaryPeriodic) {  // ghosts mirror the opposite interior node
-            xx = x == 0 ? g.NX - 2 : (x == g.NX - 1 ? 1 : x);
-            yy = y == 0 ? g.NY - 2 : (y == g.NY - 1 ? 1 : y);
-            zz = z == 0 ? g.NZ - 2 : (z == g.NZ - 1 ? 1 : z);
+            xx = wrap_interior(x, g.NX);
+            yy = wrap_interior(y, g.NY);
+            zz = wrap_interior(z, g.NZ);
         }
         const float dx = float(xx) - bx, dy = float(yy) - by, dz = float(zz) - bz;
         const float in = ((dx * dx) + (dy * dy) + (dz * dz)) <= r2 ? 1.0f : 0.0f;
@@ -599,9 +821,10 @@ __global__ void k_init_pops(const DeviceState s, int mode, const float *fr_ref, 
                 fb = fb * f;
             }
         }
-        const uint32_t src = pull_src_rt(g, x, y, z, i);
-        C::store_to(s.pops[0], g.N, i, src, fr, fb, s.ph.f16_rho0);
-        C::store_to(s.pops[1], g.N, i, src, fr, fb, s.ph.f16_rho0);
+        int xs, ys, zs;
+        pull_src_rt(g, x, y, z, i, xs, ys, zs);
+        C::store_to(s.pops[0], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
+        C::store_to(s.pops[1], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
     }
 }
 
@@ -613,9 +836,9 @@ __global__ void k_refresh_psi(const DeviceState s) {
     if (x >= g.NX || y >= g.NY) return;
     int xx = x, yy = y, zz = z;
     if (g.boundary == kBoundaryPeriodic) {
-        xx = x == 0 ? g.NX - 2 : (x == g.NX - 1 ? 1 : x);
-        yy = y == 0 ? g.NY - 2 : (y == g.NY - 1 ? 1 : y);
-        zz = z == 0 ? g.NZ - 2 : (z == g.NZ - 1 ? 1 : z);
+        xx = wrap_interior(x, g.NX);
+        yy = wrap_interior(y, g.NY);
+        zz = wrap_interior(z, g.NZ);
     }
     const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
     const uint32_t src = uint32_t(xx) + uint32_t(g.sy) * uint32_t(yy) + uint32_t(g.sz) * uint32_t(zz);
@@ -637,7 +860,11 @@ __global__ void k_gather_pops(const DeviceState s, int cur, float *fr_ref, float
     const bool interior = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
     for (int i = 0; i < kQ; ++i) {
         float fr = 0.0f, fb = 0.0f;
-        if (interior) C::load_from(s.pops[cur], g.N, i, pull_src_rt(g, x, y, z, i), fr, fb, s.ph.f16_rho0);
+        if (interior) {
+            int xs, ys, zs;
+            pull_src_rt(g, x, y, z, i, xs, ys, zs);
+            C::load_from(s.pops[cur], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
+        }
         fr_ref[size_t(i) * N + id] = fr;
         fb_ref[size_t(i) * N + id] = fb;
     }
@@ -703,8 +930,10 @@ __global__ void __launch_bounds__(kRedThreads) k_conservation_partials(const Dev
         const int x = int(id % g.NX), y = int((id / g.NX) % g.NY), z = int(id / (size_t(g.NX) * g.NY));
         if (x < 1 || x > g.NX - 2 || y < 1 || y > g.NY - 2 || z < 1 || z > g.NZ - 2) continue;
         for (int i = 0; i < kQ; ++i) {
+            int xs, ys, zs;
+            pull_src_rt(g, x, y, z, i, xs, ys, zs);
             float fr, fb;
-            C::load_from(s.pops[cur], g.N, i, pull_src_rt(g, x, y, z, i), fr, fb, s.ph.f16_rho0);
+            C::load_from(s.pops[cur], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
             const double a = fr, b = fb;
             acc[0] += a;
             acc[1] += b;
@@ -740,8 +969,10 @@ __global__ void k_check_finite(const DeviceState s, int cur, int *flag) {
         bool bad = false;
         for (int k = 0; k < kMomCount; ++k) bad |= !isfinite(s.mom[size_t(k) * N + id]);
         for (int i = 0; i < kQ; ++i) {
+            int xs, ys, zs;
+            pull_src_rt(g, x, y, z, i, xs, ys, zs);
             float fr, fb;
-            C::load_from(s.pops[cur], g.N, i, pull_src_rt(g, x, y, z, i), fr, fb, s.ph.f16_rho0);
+            C::load_from(s.pops[cur], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
             bad |= !isfinite(fr) || !isfinite(fb);
         }
         if (bad) atomicOr(flag, 1);
@@ -755,34 +986,119 @@ unsigned grid1(const Geometry &g) {
     return unsigned(want < size_t(8 * 148) ? want : size_t(8 * 148));
 }
 
+template <class C, bool kStats, bool kPeriodic>
+cudaError_t fused_attr(int smem) {
+    return cudaFuncSetAttribute(k_fused<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+template <class C, bool kStats, bool kPeriodic>
+cudaError_t fused_launch(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(t.ny_tiles, t.nz_chunks);
+    cfg.blockDim = dim3(kFusedThreads);
+    cfg.dynamicSmemBytes = size_t(t.smem_bytes);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = unsigned(t.cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_fused<C, kStats, kPeriodic>, s, t, cur, step);
+}
+
 template <class C, bool kStats>
+cudaError_t fused_dispatch(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
+    if (s.g.boundary == kBoundaryPeriodic) return fused_launch<C, kStats, true>(s, t, cur, step, st);
+    return fused_launch<C, kStats, false>(s, t, cur, step, st);
+}
+
+template <class C>
 cudaError_t moments_dispatch(const DeviceState &s, int cur, int64_t step, cudaStream_t st) {
     const C codec = make_codec<C>(s, cur);
     if (s.g.boundary == kBoundaryPeriodic)
-        k_moments<C, kStats, true><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, codec, step);
+        k_moments<C, true><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, codec, step);
     else
-        k_moments<C, kStats, false><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, codec, step);
+        k_moments<C, false><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, codec, step);
     return cudaGetLastError();
 }
 
 template <class C>
-cudaError_t moments_stats(const DeviceState &s, int cur, int64_t step, bool stats, cudaStream_t st) {
-    return stats ? moments_dispatch<C, true>(s, cur, step, st) : moments_dispatch<C, false>(s, cur, step, st);
-}
-
-template <class C>
-cudaError_t boundary_dispatch(const DeviceState &s, int wbuf, int64_t step, int which, cudaStream_t st) {
+cudaError_t boundary_dispatch(const DeviceState &s, int wbuf, int64_t step, int which, bool from_bmom,
+                              cudaStream_t st) {
     dim3 grid = grid_plane(s.g);
     grid.z = which >= 0 ? 1 : 2;
-    k_boundary<C><<<grid, dim3(32, 8), 0, st>>>(s, wbuf, step, which);
+    k_boundary<C><<<grid, dim3(32, 8), 0, st>>>(s, wbuf, step, which, from_bmom ? 1 : 0);
     return cudaGetLastError();
 }
 
 }  // namespace
 
+// ---------------------------------------------------------------------- host side
+
+FusedTiling fused_tiling(const Geometry &g, int max_smem) {
+    FusedTiling t{};
+    t.tpr = ((g.NX + 31) / 32) * 32;
+    const int per_row = t.tpr * 4;
+    const int rpt = kFusedThreads / t.tpr;
+    // rows per tile: at least one round of rows in parallel, 4 by default
+    // (measured best on 128x256x128), fewer if shared memory
+    // (3*(ty+2) + 2*11*ty) * tpr * 4 bytes does not fit
+    int ty = std::max(4, rpt);
+    if (const char *v = std::getenv("MCG_FUSED_TY")) ty = std::max(1, std::atoi(v));  // tuning sweeps
+    while (ty > 1 && (3 * (ty + 2) + 2 * kMomCount * ty) * per_row > max_smem) --ty;
+    if (ty > rpt) ty -= ty % rpt;  // whole rounds of rows in parallel
+    t.ty = ty;
+    t.ny_tiles = (g.NY - 2 + ty - 1) / ty;
+    // y-tiles per cluster: 1 by default (measured: sharing halo rows through
+    // distributed shared memory cost more in cluster barriers than it saved in
+    // pulls on 128x256x128); the cluster path stays selectable for tuning
+    t.cluster = 1;
+    if (const char *v = std::getenv("MCG_FUSED_CLUSTER")) {  // tuning sweeps
+        const int c = std::atoi(v);
+        if (c >= 1 && c <= 8 && t.ny_tiles % c == 0) t.cluster = c;
+    }
+    // z chunks: about seven CTAs per SM over the launch (measured best: 8-plane
+    // chunks, 1024 CTAs on 128x256x128)
+    const int target = 7 * 148;
+    int chunks = (target + t.ny_tiles - 1) / t.ny_tiles;
+    if (chunks < 1) chunks = 1;
+    int lz = (g.NZ - 2 + chunks - 1) / chunks;
+    if (lz < 4) lz = 4;
+    if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
+    t.lz = lz;
+    t.nz_chunks = (g.NZ - 2 + lz - 1) / lz;
+    t.smem_bytes = (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
+    return t;
+}
+
+cudaError_t fused_configure(int smem) {
+    cudaError_t e;
+    if ((e = fused_attr<CodecF32, false, false>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF32, true, false>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF32, false, true>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF32, true, true>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF16, false, false>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF16, true, false>(smem)) != cudaSuccess) return e;
+    if ((e = fused_attr<CodecF16, false, true>(smem)) != cudaSuccess) return e;
+    return fused_attr<CodecF16, true, true>(smem);
+}
+
+cudaError_t launch_fused(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, bool stats,
+                         cudaStream_t st) {
+    if (s.g.storage == kStoreF16)
+        return stats ? fused_dispatch<CodecF16, true>(s, t, cur, step, st)
+                     : fused_dispatch<CodecF16, false>(s, t, cur, step, st);
+    return stats ? fused_dispatch<CodecF32, true>(s, t, cur, step, st)
+                 : fused_dispatch<CodecF32, false>(s, t, cur, step, st);
+}
+
 cudaError_t launch_moments(const DeviceState &s, int cur, int64_t step, bool stats, cudaStream_t st) {
-    if (s.g.storage == kStoreF16) return moments_stats<CodecF16>(s, cur, step, stats, st);
-    return moments_stats<CodecF32>(s, cur, step, stats, st);
+    cudaError_t e = s.g.storage == kStoreF16 ? moments_dispatch<CodecF16>(s, cur, step, st)
+                                             : moments_dispatch<CodecF32>(s, cur, step, st);
+    if (e != cudaSuccess || !stats) return e;
+    return launch_accumulate_radial(s, st);
 }
 
 cudaError_t launch_collide(const DeviceState &s, int cur, int64_t step, cudaStream_t st) {
@@ -793,9 +1109,10 @@ cudaError_t launch_collide(const DeviceState &s, int cur, int64_t step, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int which, cudaStream_t st) {
-    if (s.g.storage == kStoreF16) return boundary_dispatch<CodecF16>(s, wbuf, step, which, st);
-    return boundary_dispatch<CodecF32>(s, wbuf, step, which, st);
+cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int which, bool from_bmom,
+                            cudaStream_t st) {
+    if (s.g.storage == kStoreF16) return boundary_dispatch<CodecF16>(s, wbuf, step, which, from_bmom, st);
+    return boundary_dispatch<CodecF32>(s, wbuf, step, which, from_bmom, st);
 }
 
 cudaError_t launch_accumulate_radial(const DeviceState &s, cudaStream_t st) {
@@ -804,7 +1121,7 @@ cudaError_t launch_accumulate_radial(const DeviceState &s, cudaStream_t st) {
 }
 
 cudaError_t launch_init_fields(const DeviceState &s, int mode, int red_inside, float r2, float bx, float by, float bz,
-                               float, cudaStream_t st) {
+                               cudaStream_t st) {
     k_init_fields<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, mode, red_inside, r2, bx, by, bz);
     return cudaGetLastError();
 }

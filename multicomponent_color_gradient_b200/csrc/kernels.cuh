@@ -1,20 +1,28 @@
 // kernels.cuh - device-side data layout and kernel entry points of the step.
 //
-// HBM layout (all structure-of-arrays, node index id = x + NX*(y + NY*z)):
-//   pops[2]   two population buffers (ping-pong).  A buffer holds, at node s
-//             and direction i, the value that streams OUT of s along c_i
-//             (post-collision, pull layout): node x reads f_i(x) from
-//             src(x,i) = x - c_i.  The y ghost planes hold what the boundary
+// HBM layout (node index id = x + NX*(y + NY*z) for the per-node fields):
+//   pops[2]   two population buffers (ping-pong), row-blocked: row (y,z) holds
+//             `slots` x-rows of NX values, grouped by pull source (lattice.cuh
+//             slot_f32 / slot_f16); element (slot, x, y, z) is at
+//             ((z*NY + y)*slots + slot)*NX + x.
+//             A buffer holds, at node s and direction i, the value that streams
+//             OUT of s along c_i (post-collision, pull layout): node x reads
+//             f_i(x) from x - c_i.  The y ghost planes hold what the boundary
 //             delivers into the first/last fluid plane.
-//               F32: float  [2 colours][27][N]
-//               F16: __half2[27][N] = (total offset by w_i*rho0 over w_i,
-//                                      colour fraction (fr-fb)/(fr+fb))
+//               F32: float,   slots = 54 (27 directions x 2 colours)
+//               F16: __half2, slots = 27 ((total offset by w_i*rho0)/w_i,
+//                                         signed minority-colour fraction)
 //   mom       11 float planes [11][N]: rr, rb, ux, uy, uz, Pixx, Pixy, Piyy,
 //             Piyz, Pizz, Pixz - the reference's LbmDevice fields
-//             (memory.cuh:11-25), ghost nodes included.
+//             (memory.cuh:11-25), ghost nodes included.  The fused step does
+//             not stream them; they are refreshed on demand (output steps,
+//             granular launch sequence).
 //   psi[2]    colour field psi = (rr-rb)/(rr+rb) per node, ping-pong by step
-//             parity; ghost nodes carry what the reference's unwrapped
-//             colour-gradient stencil reads there (forces.cuh:31-33).
+//             parity; the fused step reads only its ghost nodes, which carry
+//             what the reference's unwrapped colour-gradient stencil reads
+//             there (forces.cuh:31-33).
+//   bmom      moments of the first and last fluid planes (y=1, y=NY-2),
+//             [2][NZ][11][NX], for the boundary launch.
 #pragma once
 
 #include <cstddef>
@@ -29,11 +37,19 @@ enum : int { kMomRR = 0, kMomRB, kMomUX, kMomUY, kMomUZ, kMomPXX, kMomPXY, kMomP
 
 struct Geometry {
     int NX, NY, NZ;
-    uint32_t N;  // NX*NY*NZ (< 2^32)
-    int sy, sz;  // strides of y and z: NX, NX*NY
+    uint32_t N;  // NX*NY*NZ (< 2^31)
+    int sy, sz;  // strides of y and z in the per-node fields: NX, NX*NY
     int boundary;
     int storage;
+    int slots;   // x-rows per lattice row in the population buffers (54 or 27)
 };
+
+__host__ __device__ __forceinline__ size_t pop_row(const Geometry &g, int y, int z) {
+    return (size_t(z) * size_t(g.NY) + size_t(y)) * size_t(g.slots) * size_t(g.NX);
+}
+__host__ __device__ __forceinline__ size_t pop_index(const Geometry &g, int slot, int x, int y, int z) {
+    return pop_row(g, y, z) + size_t(slot) * size_t(g.NX) + size_t(x);
+}
 
 struct Physics {
     float omega;          // bulk relaxation rate omega_sponge(y) when sponge_K == 0 (mathUtilities.cuh:60-90)
@@ -49,8 +65,20 @@ struct Physics {
     float nu, sponge_K, sponge_y_start, sponge_inv_width;
     // radial statistics
     int NRB;
-    // F16 storage: populations are stored as (g/w - rho0) and (fr-fb)/g
+    // F16 storage: populations are stored as (g/w - rho0) and the colour fraction
     float f16_rho0;
+};
+
+// Tiling of the fused step: a CTA owns rows [y0, y0+ty) of every plane of a
+// z-chunk [z0, z0+lz) and marches z; tpr threads per row (a multiple of 32,
+// >= NX), blockDim.x / tpr rows in parallel.  `cluster` consecutive y-tiles
+// form a thread-block cluster that exchanges edge psi rows through
+// distributed shared memory, so only the cluster's outer halo rows are pulled.
+struct FusedTiling {
+    int ty, lz, tpr;
+    int ny_tiles, nz_chunks;
+    int cluster;
+    int smem_bytes;
 };
 
 struct DeviceState {
@@ -59,6 +87,7 @@ struct DeviceState {
     void *pops[2];
     float *mom;       // [11][N]
     float *psi[2];    // [N] each
+    float *bmom;      // [2][NZ][11][NX]
     double *radial;   // [5][NY*NRB]
     float *uy_avg;    // [N]
     double *partials; // reduction scratch
@@ -66,19 +95,27 @@ struct DeviceState {
     int *flag;        // device flag (non-finite detection)
 };
 
-// Launch helpers; all return cudaGetLastError() of the launch.
+// ---- the fused step (moments + colour gradient + collision in one pass) ----
+FusedTiling fused_tiling(const Geometry &g, int max_smem_per_block);
+cudaError_t fused_configure(int max_smem);
+cudaError_t launch_fused(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, bool stats,
+                         cudaStream_t st);
+
+// ---- granular launch sequence (launch.cuh order) ----
 // step: the reference loop index of the step being computed.
 cudaError_t launch_moments(const DeviceState &s, int cur, int64_t step, bool stats, cudaStream_t st);
 cudaError_t launch_collide(const DeviceState &s, int cur, int64_t step, cudaStream_t st);
-// Jet inlet (which=0), outlet (1) or both (-1) of step `step`, from the moments
-// of that step, into the ghost planes of pops[wbuf] and psi[(step+1)&1].
-cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int which, cudaStream_t st);
+// Jet inlet (which=0), outlet (1) or both (-1) of step `step`, into the ghost
+// planes of pops[wbuf] and psi[(step+1)&1].  from_bmom: moments of the fluid
+// planes come from bmom (fused step) instead of mom (granular sequence).
+cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int which, bool from_bmom,
+                            cudaStream_t st);
 cudaError_t launch_accumulate_radial(const DeviceState &s, cudaStream_t st);
 
 // Initial state.  mode 0: jet (jet/jetIn.cuh), 1: bubble (bubble/bubbleIn.cuh),
 // 2: populations from reference-layout device arrays fr_ref/fb_ref.
 cudaError_t launch_init_fields(const DeviceState &s, int mode, int red_inside, float bubble_r2, float bx, float by,
-                               float bz, float noise, cudaStream_t st);
+                               float bz, cudaStream_t st);
 cudaError_t launch_init_pops(const DeviceState &s, int mode, const float *fr_ref, const float *fb_ref, float noise,
                              cudaStream_t st);
 // psi of both buffers from the density planes, all nodes (periodic: ghosts mirrored).

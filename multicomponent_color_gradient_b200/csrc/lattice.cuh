@@ -77,6 +77,14 @@ struct Dir {
 // Opposite direction of i in the reference order (pairs 2k-1, 2k).
 __host__ __device__ constexpr int dir_opp(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
 
+// Row-blocked population layout.  All populations of one lattice row (y,z)
+// are contiguous; inside a row they are grouped by the row they are pulled
+// from: group g = (cy+1)*3 + (cz+1), then colour, then cx.  A pulled row is
+// therefore 9 contiguous segments of 6 x-rows (float32) or 3 (float16 pairs).
+__host__ __device__ constexpr int dir_group(int i) { return (dir_cy(i) + 1) * 3 + (dir_cz(i) + 1); }
+__host__ __device__ constexpr int slot_f32(int i, int colour) { return dir_group(i) * 6 + colour * 3 + (dir_cx(i) + 1); }
+__host__ __device__ constexpr int slot_f16(int i) { return dir_group(i) * 3 + (dir_cx(i) + 1); }
+
 template <int... Is, class F>
 __device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, Is...>) {
     (f(std::integral_constant<int, Is>{}), ...);
@@ -149,6 +157,43 @@ __device__ __forceinline__ float fneq(const NeqTerms &n) {
     if constexpr (D::Hyzz != 0.0f) A3 += n.a3yzz * D::Hyzz;
     if constexpr (D::Hxyz != 0.0f) A3 += 2.0f * n.a3xyz * D::Hxyz;
     return D::w * (A2 + A3 * kInv2Cs6);
+}
+
+// Directions 2k-1 and 2k are opposite (stencil_ct.cuh:9-16).  For such a pair
+// the equilibrium and the regularised non-equilibrium split into a part even
+// in c (same for both) and a part odd in c (sign flips), so one evaluation
+// serves both directions.  feq_i = w rho (E + O), feq_ibar = w rho (E - O);
+// fneq_i = w (A2 + A3), fneq_ibar = w (A2 - A3).
+template <int I>
+__device__ __forceinline__ void feq_pair(float rho, const EqTerms &e, float &fi, float &fo) {
+    using D = Dir<I>;
+    float cu = 0.0f;
+    if constexpr (D::cx != 0) cu += D::fx * e.ux;
+    if constexpr (D::cy != 0) cu += D::fy * e.uy;
+    if constexpr (D::cz != 0) cu += D::fz * e.uz;
+    const float even = 1.0f + ((cu * cu) * kInv2Cs4 - e.usq * kInv2Cs2);
+    const float odd = cu * kInvCs2 + cu * ((cu * cu) * kInv6Cs6 - e.usq * kInv2Cs4);
+    const float wr = D::w * rho;
+    fi = wr * (even + odd);
+    fo = wr * (even - odd);
+}
+
+template <int I>
+__device__ __forceinline__ void fneq_pair(const NeqTerms &n, float &fi, float &fo) {
+    using D = Dir<I>;
+    const float A2 = (n.pxx * D::Hxx + 2.0f * n.pxy * D::Hxy + n.pyy * D::Hyy + 2.0f * n.pyz * D::Hyz +
+                      n.pzz * D::Hzz + 2.0f * n.pxz * D::Hxz) * kInv2Cs4;
+    float A3 = 0.0f;
+    if constexpr (D::Hxxy != 0.0f) A3 += n.a3xxy * D::Hxxy;
+    if constexpr (D::Hxxz != 0.0f) A3 += n.a3xxz * D::Hxxz;
+    if constexpr (D::Hxyy != 0.0f) A3 += n.a3xyy * D::Hxyy;
+    if constexpr (D::Hxzz != 0.0f) A3 += n.a3xzz * D::Hxzz;
+    if constexpr (D::Hyyz != 0.0f) A3 += n.a3yyz * D::Hyyz;
+    if constexpr (D::Hyzz != 0.0f) A3 += n.a3yzz * D::Hyzz;
+    if constexpr (D::Hxyz != 0.0f) A3 += 2.0f * n.a3xyz * D::Hxyz;
+    A3 *= kInv2Cs6;
+    fi = D::w * (A2 + A3);
+    fo = D::w * (A2 - A3);
 }
 
 // Interface terms shared by all directions of one node.

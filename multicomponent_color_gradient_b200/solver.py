@@ -132,11 +132,11 @@ class Solver:
         return float(ms.value)
 
     def step_profiled(self, nsteps: int):
-        """(total ms, {moments, boundary, collide} ms) with an event between launches."""
+        """(total ms, {fused, boundary} ms) with an event between launches."""
         tot = C.c_float()
         ks = (C.c_float * 3)()
         self._c("mcg_step_profiled", int(nsteps), C.byref(tot), ks)
-        return float(tot.value), {"moments": ks[0], "boundary": ks[1], "collide": ks[2]}
+        return float(tot.value), {"fused": ks[0], "boundary": ks[1]}
 
     @property
     def current_step(self) -> int:
