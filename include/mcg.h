@@ -242,6 +242,39 @@ mcg_status mcg_check_finite(mcg_handle *h);
 mcg_status mcg_conservation_sums_static(const float *fr, const float *fb, int32_t NX, int32_t NY, int32_t NZ,
                                         double *out5, void *stream);
 
+/* ---------------- discrete adjoint (no counterpart in the reference) ---------------- */
+
+/* Initial state with a velocity field: every interior node gets, per colour,
+ * the third-order equilibrium feq_i(rho_c, u) of lbm.cuh:16-35 (the
+ * reference's bubble and jet initial states are the u = 0 case,
+ * bubble/bubbleIn.cuh:25-39).  Host arrays of Ncells floats; resets the step
+ * counter like mcg_init_bubble. */
+mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *rhob,
+                                const float *ux, const float *uy, const float *uz);
+
+/* Discrete adjoint of nsteps steps of the periodic box (boundary
+ * MCG_BOUNDARY_PERIODIC, float32 storage) from the handle's current state S_0,
+ * for J = sum over interior nodes of (psi_T - psi_target)^2, where psi_T is the
+ * colour field of the populations after nsteps steps (what mcg_get_populations
+ * returns then).  Reverse sweep with binomial checkpointing in device memory:
+ * `snapshots` states are held (S_0 in the handle's own buffer, snapshots-1 more
+ * allocated for the call), recomputing forward segments as Griewank's
+ * treeverse schedule prescribes.  psi_target: host, Ncells floats (reference
+ * node order).  Outputs (any may be NULL): J; dJ/dsigma and dJ/dtau (tau =
+ * taur = taub, nu = (tau - 1/2) cs^2); dJ_du0: host, 3*Ncells floats (ux, uy,
+ * uz planes, ghost nodes 0) - the gradient with respect to the velocity u0 of
+ * an initial state made by mcg_init_equilibrium; forward_steps: fused steps run
+ * (recomputation included); ms: device time of the call.  The handle's state,
+ * fields and step counter are left as they were. */
+mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nsteps, int32_t snapshots,
+                           double *J, double *dJ_dsigma, double *dJ_dtau, float *dJ_du0,
+                           int64_t *forward_steps, float *ms);
+/* The treeverse schedule without running it (host only, no device needed):
+ * fused steps a reverse sweep over nsteps steps with `snapshots` held states
+ * runs, and the recomputation depth r (least r with C(s + r, s) >= nsteps + 1,
+ * s = min(snapshots, nsteps + 1)). */
+mcg_status mcg_adjoint_plan(int32_t nsteps, int32_t snapshots, int64_t *forward_steps, int32_t *sweeps);
+
 /* ---------------- output files (io/save_data.cuh, meanF/meanFieldsRT.cuh) ---------------- */
 
 /* initialize_mean_fields_runtime (meanF/meanFieldsRT.cuh:132-162): creates

@@ -1,0 +1,277 @@
+// adjoint.cu - discrete adjoint of the periodic-box step (mcg_adjoint_run and
+// mcg_adjoint_plan in include/mcg.h).
+//
+// The reverse sweep visits the states S_T, S_{T-1}, ..., S_0 of a T-step run.
+// Op t (t = T: terminal condition of J; t < T: one adjoint step
+// lambda_{t+1} -> lambda_t) needs S_t, so a sweep is n = T + 1 ops over a
+// chain whose states can only be made going forward.  The schedule is
+// Griewank's binomial checkpointing (treeverse): with s held states (the
+// segment's first included) and r recomputation sweeps, beta(s, r) =
+// C(s + r, s) ops can be reversed.  A segment of n ops is split at m: advance
+// m steps into a free slot, reverse the right part n - m with s - 1 held
+// states, then the left part m with s.  r is least with beta(s, r) >= n and
+// m = max(n - beta(s - 1, r), beta(s, r - 2), 1), the lower end of the range
+// of splits that reach the fewest forward steps, r n - beta(s + 1, r - 1).
+// With s >= n every state is made once (T forward steps).
+//
+// Snapshots are full population buffers in HBM.  Forward steps write straight
+// into the next slot (or ping-pong through two work buffers for longer
+// segments), so no state is ever copied.  The run's moment planes and colour
+// fields live in their own buffers: the handle's state is left untouched.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.hpp"
+#include "lattice.cuh"
+
+using mcg::cuda_fail;
+using mcg::fail;
+
+namespace {
+
+// beta(s, r) = C(s + r, s) (0 for r < 0), saturated well above any step count
+int64_t beta(int64_t s, int64_t r) {
+    if (r < 0) return 0;
+    const int64_t cap = int64_t(1) << 40;
+    int64_t b = 1;
+    for (int64_t k = 1; k <= r; ++k) {
+        b = b * (s + k) / k;  // C(s+k, k) = C(s+k-1, k-1) * (s+k) / k, exact
+        if (b > cap) return cap;
+    }
+    return b;
+}
+
+// least r with beta(s, r) >= n, s >= 1 held states
+int least_sweeps(int64_t n, int64_t s) {
+    int r = 0;
+    while (beta(s, r) < n) ++r;
+    return r;
+}
+
+// One action of the schedule.
+struct Action {
+    enum Kind { kAdvance, kAdjoint } kind;
+    int src;      // slot holding the first state (kAdvance) / the op's state (kAdjoint, -1: last advance's result)
+    int dst;      // kAdvance: destination slot, -1 for a work buffer
+    int64_t t0;   // time of the source state / of the op
+    int64_t n;    // steps (kAdvance)
+};
+
+void plan(std::vector<Action> &out, int64_t t0, int64_t n, int slot, int free_slots) {
+    if (n <= 0) return;
+    if (n == 1) {
+        out.push_back({Action::kAdjoint, slot, -1, t0, 0});
+        return;
+    }
+    if (free_slots == 0) {
+        for (int64_t k = n - 1; k >= 1; --k) {
+            out.push_back({Action::kAdvance, slot, -1, t0, k});
+            out.push_back({Action::kAdjoint, -1, -1, t0 + k, 0});
+        }
+        out.push_back({Action::kAdjoint, slot, -1, t0, 0});
+        return;
+    }
+    const int64_t held = free_slots + 1;
+    const int r = least_sweeps(n, held);
+    int64_t m = std::max<int64_t>(std::max<int64_t>(n - beta(held - 1, r), beta(held, r - 2)), 1);
+    if (m > n - 1) m = n - 1;
+    out.push_back({Action::kAdvance, slot, slot + 1, t0, m});
+    plan(out, t0 + m, n - m, slot + 1, free_slots - 1);
+    plan(out, t0, m, slot, free_slots);
+}
+
+int64_t forward_steps_of(const std::vector<Action> &acts) {
+    int64_t f = 0;
+    for (const Action &a : acts)
+        if (a.kind == Action::kAdvance) f += a.n;
+    return f;
+}
+
+#define ADJ_CUDA(call, what)                                 \
+    do {                                                     \
+        cudaError_t e__ = (call);                            \
+        if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+    } while (0)
+
+#define ADJ_LAUNCH(h, call, what)                            \
+    do {                                                     \
+        cudaError_t e__ = (call);                            \
+        if (e__ != cudaSuccess) return cuda_fail(e__, what); \
+        ++(h)->launches;                                     \
+    } while (0)
+
+struct DeviceBuffers {
+    std::vector<void *> ptrs;
+    ~DeviceBuffers() {
+        for (void *p : ptrs) cudaFree(p);
+    }
+    cudaError_t alloc(void **p, size_t bytes) {
+        *p = nullptr;
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) return e;
+        ptrs.push_back(*p);
+        return cudaMemsetAsync(*p, 0, bytes);
+    }
+};
+
+struct Run {
+    mcg_handle *h = nullptr;
+    mcg::DeviceState base{};   // the handle's state with the run's own moment / psi planes
+    std::vector<void *> slots; // slots[0] = S_0 (the handle's buffer)
+    void *work[2] = {nullptr, nullptr};
+    float *lam[2] = {nullptr, nullptr};
+    int lc = 0;                // lam[lc]: adjoint of the latest state reached
+    float *lmom = nullptr, *lf = nullptr;
+    const float *target = nullptr;
+    double *acc = nullptr;     // [0] J, [1] dJ/domega, [2] dJ/d(A/2)
+    int64_t step0 = 0, T = 0;
+
+    mcg::DeviceState with(void *from, void *to) const {
+        mcg::DeviceState d = base;
+        d.pops[0] = from;
+        d.pops[1] = to;
+        return d;
+    }
+
+    // S_{t0+n} from S_{t0} (in `src`) into `dst`, or into a work buffer when dst
+    // is null; returns the buffer holding the result.
+    mcg_status advance(void *src, void *dst, int64_t t0, int64_t n, void **result) {
+        void *a = src;
+        for (int64_t k = 0; k < n; ++k) {
+            void *b = (k == n - 1 && dst) ? dst : work[k & 1];
+            ADJ_LAUNCH(h, mcg::launch_fused(with(a, b), h->tiling, 0, step0 + t0 + k, false, h->stream),
+                       "adjoint: forward step");
+            a = b;
+        }
+        *result = a;
+        return MCG_OK;
+    }
+
+    // op t on the state held in `state`
+    mcg_status op(void *state, int64_t t) {
+        const mcg::DeviceState d = with(state, nullptr);
+        ADJ_LAUNCH(h, mcg::launch_moments(d, 0, step0 + t, false, h->stream), "adjoint: moments");
+        if (t == T) {
+            ADJ_LAUNCH(h, mcg::launch_adj_terminal(d, target, lam[lc], acc, h->stream), "adjoint: terminal");
+        } else {
+            ADJ_LAUNCH(h, mcg::launch_adj_step(d, step0 + t, lam[lc], lmom, lf, lam[lc ^ 1], acc + 1, h->stream),
+                       "adjoint: step");
+            h->launches += 1;  // two kernels
+            lc ^= 1;
+        }
+        return MCG_OK;
+    }
+
+    mcg_status execute(const std::vector<Action> &acts) {
+        void *last = nullptr;
+        for (const Action &a : acts) {
+            if (a.kind == Action::kAdvance) {
+                void *dst = a.dst >= 0 ? slots[size_t(a.dst)] : nullptr;
+                if (mcg_status s = advance(slots[size_t(a.src)], dst, a.t0, a.n, &last)) return s;
+            } else {
+                void *state = a.src >= 0 ? slots[size_t(a.src)] : last;
+                if (mcg_status s = op(state, a.t0)) return s;
+            }
+        }
+        return MCG_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+mcg_status mcg_adjoint_plan(int32_t nsteps, int32_t snapshots, int64_t *forward_steps, int32_t *sweeps) {
+    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+    if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
+    const int free_slots = std::min<int64_t>(snapshots - 1, nsteps);
+    std::vector<Action> acts;
+    plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
+    if (forward_steps) *forward_steps = forward_steps_of(acts);
+    if (sweeps) *sweeps = least_sweeps(int64_t(nsteps) + 1, free_slots + 1);
+    return MCG_OK;
+}
+
+mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nsteps, int32_t snapshots, double *J,
+                           double *dJ_dsigma, double *dJ_dtau, float *dJ_du0, int64_t *forward_steps, float *ms) {
+    if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+    if (!psi_target) return fail(MCG_ERR_INVALID_ARG, "psi_target is null");
+    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+    if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
+    if (h->p.boundary != MCG_BOUNDARY_PERIODIC || h->p.storage != MCG_STORAGE_F32)
+        return fail(MCG_ERR_UNSUPPORTED, "the adjoint covers the periodic box with float32 storage");
+    if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
+    const mcg::Geometry &g = h->s.g;
+    const size_t N = g.N;
+    const size_t pop_bytes = size_t(g.slots) * N * sizeof(float);
+    const int free_slots = int(std::min<int64_t>(snapshots - 1, nsteps));
+
+    std::vector<Action> acts;
+    plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
+
+    DeviceBuffers buf;
+    Run run;
+    run.h = h;
+    run.base = h->s;
+    run.step0 = h->step;
+    run.T = nsteps;
+    run.slots.assign(size_t(free_slots) + 1, nullptr);
+    run.slots[0] = h->s.pops[h->cur];
+    void *p = nullptr;
+    for (int k = 1; k <= free_slots; ++k) {
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint snapshot slots");
+        run.slots[size_t(k)] = p;
+    }
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint work buffers");
+        run.work[k] = p;
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint lambda buffers");
+        run.lam[k] = static_cast<float *>(p);
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment planes");
+    run.base.mom = static_cast<float *>(p);
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "adjoint psi planes");
+        run.base.psi[k] = static_cast<float *>(p);
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment adjoints");
+    run.lmom = static_cast<float *>(p);
+    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint gradient adjoints");
+    run.lf = static_cast<float *>(p);
+    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint du0");
+    float *du0 = static_cast<float *>(p);
+    ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "adjoint target");
+    run.target = static_cast<const float *>(p);
+    ADJ_CUDA(cudaMemcpyAsync(p, psi_target, N * sizeof(float), cudaMemcpyHostToDevice, h->stream), "upload target");
+    ADJ_CUDA(buf.alloc(&p, 4 * sizeof(double)), "adjoint accumulators");
+    run.acc = static_cast<double *>(p);
+
+    ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
+    if (mcg_status s = run.execute(acts)) return s;
+    // op 0 left the moments of S_0 in the run's planes
+    ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
+    ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
+    double acc[3] = {0, 0, 0};
+    ADJ_CUDA(cudaMemcpyAsync(acc, run.acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream), "download J");
+    if (dJ_du0)
+        ADJ_CUDA(cudaMemcpyAsync(dJ_du0, du0, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+                 "download dJ/du0");
+    ADJ_CUDA(cudaStreamSynchronize(h->stream), "adjoint run");
+    float t_ms = 0.f;
+    ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
+
+    // omega = 1/(1/2 + nu/cs^2) = 1/tau; A/2 = sigma / (8 cs^4 taub)
+    const double omega = h->s.ph.omega, Ah = h->s.ph.Ah;
+    const double tau = h->p.taub;
+    const double dAh_dsigma = 1.0 / (8.0 * double(mcg::kCs4) * tau);
+    if (J) *J = acc[0];
+    if (dJ_dsigma) *dJ_dsigma = acc[2] * dAh_dsigma;
+    if (dJ_dtau) *dJ_dtau = acc[1] * (-omega * omega) + acc[2] * (-Ah / tau);
+    if (forward_steps) *forward_steps = forward_steps_of(acts);
+    if (ms) *ms = t_ms;
+    return MCG_OK;
+}
+
+}  // extern "C"

@@ -416,6 +416,17 @@ mcg_status mcg_init_bubble(mcg_handle *h) {
     return init_common(h, 1);
 }
 
+mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *rhob, const float *ux,
+                                const float *uy, const float *uz) {
+    if (mcg_status s = check_handle(h)) return s;
+    MCG_REQUIRE(rhor && rhob && ux && uy && uz, "field pointers must not be null");
+    if (mcg_status s = reset_counters(h)) return s;
+    if (mcg_status s = mcg_set_fields(h, rhor, rhob, ux, uy, uz)) return s;
+    MCG_LAUNCH(h, mcg::launch_init_pops(h->s, 3, nullptr, nullptr, 0.0f, h->stream), "equilibrium populations");
+    MCG_CUDA(cudaStreamSynchronize(h->stream), "init equilibrium");
+    return MCG_OK;
+}
+
 // ---------------------------------------------------------------- state transfer
 
 namespace {

@@ -804,11 +804,21 @@ __global__ void k_init_pops(const DeviceState s, int mode, const float *fr_ref, 
     const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
     const size_t N = g.N;
     const float rr = s.mom[kMomRR * N + id], rb = s.mom[kMomRB * N + id];
+    const float ux = s.mom[kMomUX * N + id], uy = s.mom[kMomUY * N + id], uz = s.mom[kMomUZ * N + id];
+    const float usq = ux * ux + uy * uy + uz * uz;
     for (int i = 0; i < kQ; ++i) {
         float fr, fb;
         if (mode == 2) {
             fr = fr_ref[size_t(i) * N + id];
             fb = fb_ref[size_t(i) * N + id];
+        } else if (mode == 3) {
+            // per colour, the third-order equilibrium at the node's velocity (lbm.cuh:16-35)
+            const float cu = float(dir_cx(i)) * ux + float(dir_cy(i)) * uy + float(dir_cz(i)) * uz;
+            const float A2 = (cu * cu) * kInv2Cs4 - usq * kInv2Cs2 + cu * kInvCs2;
+            const float A3 = cu * ((cu * cu) * kInv6Cs6 - usq * kInv2Cs4);
+            const float e = dir_w(i) * (1.0f + A2 + A3);
+            fr = e * rr;
+            fb = e * rb;
         } else {
             // jetDensity: feq(rho, 0) = w rho; bubble: w rho (jetIn.cuh:26-34, bubbleIn.cuh:25-39)
             const float w = dir_w(i);
@@ -1033,6 +1043,356 @@ cudaError_t boundary_dispatch(const DeviceState &s, int wbuf, int64_t step, int 
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ discrete adjoint
+
+// Adjoint of one step of the periodic box, float32 populations.  The forward
+// step maps the stored post-collision values S_t to S_{t+1}:
+//   f_i(x) = S_t,i(x - c_i); M(x) = moments(f(x)); psi(x) = psi(M(x));
+//   F(x) = (1/cs2) sum_j w_j c_j psi(x + c_j);  S_{t+1},i(x) = C_i(M(x), F(x)).
+// Given lambda_{t+1} = dJ/dS_{t+1} the adjoint forms lambda_t = dJ/dS_t in two
+// node-parallel passes: k_adj_collide takes C's Jacobian (moments and F of the
+// node), k_adj_moments gathers the F-adjoints of the neighbours into the
+// node's psi-adjoint, goes back through the moments and scatters along the
+// transposed streaming.  The bulk/interface switch (I <= 1e-4) and the
+// |F| <= 1e-4 cut-off are taken as in the forward step (derivatives inside
+// the branch the forward state selects).
+
+__device__ __forceinline__ double block_sum_any(double v, double *sh, int nthreads) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+    const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = t & 31, wid = t >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (t == 0)
+        for (int k = 0; k < nthreads / 32; ++k) r += sh[k];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ float lam_load(const float *lam, const Geometry &g, int slot, int x, int y, int z) {
+    return lam[pop_index(g, slot, x, y, z)];
+}
+
+// J = sum over interior nodes of (psi_T - psi*)^2 and lambda_T = dJ/dS_T.
+__global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s, const float *__restrict__ target,
+                                                           float *lam, double *J) {
+    __shared__ double sh[kBX * kBY / 32];
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    const bool in = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
+    double jloc = 0.0;
+    if (in) {
+        const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+        const size_t N = g.N;
+        const float rr = s.mom[kMomRR * N + id], rb = s.mom[kMomRB * N + id];
+        const float rho = rr + rb;
+        const float d = (rr - rb) / rho - target[id];
+        jloc = double(d) * double(d);
+        const float lpsi = 2.0f * d;
+        const float inv2 = 1.0f / (rho * rho);
+        const float lrr = lpsi * 2.0f * rb * inv2, lrb = -lpsi * 2.0f * rr * inv2;
+        const PullMap<CodecF32> pm(g, x, y, z, true);
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            size_t grow;
+            int xs;
+            pm.template src<i>(x, grow, xs);
+            lam[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrr;
+            lam[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrb;
+        });
+    }
+    const double r = block_sum_any(jloc, sh, kBX * kBY);
+    if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(J, r);
+}
+
+// Per node: lambda_post (54 values at the node) -> adjoints of the node's
+// moments (11, to lmom) and colour gradient (3, to lf); float64 partials of
+// dJ/domega (acc[0]) and dJ/d(A/2) (acc[1]).
+__global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, int64_t step, const float *lam,
+                                                          float *lmom, float *lf, double *acc) {
+    __shared__ double sh[kBX * kBY / 32];
+    const Geometry &g = s.g;
+    const Physics &ph = s.ph;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    const bool in = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
+    double a_omega = 0.0, a_Ah = 0.0;
+    if (in) {
+        const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+        const size_t N = g.N;
+        const float *mom = s.mom;
+        const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
+        const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
+        const NeqTerms n = make_neq(mom[kMomPXX * N + id], mom[kMomPXY * N + id], mom[kMomPYY * N + id],
+                                    mom[kMomPYZ * N + id], mom[kMomPZZ * N + id], mom[kMomPXZ * N + id], ux, uy, uz);
+        const EqTerms e = make_eq(ux, uy, uz);
+        const float rho = rr + rb;
+        const float invr = 1.0f / rho;
+        const float aR = rr * invr, aB = rb * invr;
+        const float oms = 1.0f - omega_at(ph, y);
+        const bool interface = !(4.0f * rr * rb * invr * invr <= 1e-4f);
+        float Fx = 0.f, Fy = 0.f, Fz = 0.f, absF = 0.f, K = 0.f;
+        bool has_dir = false;
+        if (interface) {
+            const float *psi = s.psi[step & 1];
+            float sx = 0.f, sy = 0.f, sz = 0.f;
+            static_for<kQ - 1>([&](auto I) {
+                constexpr int i = decltype(I)::value + 1;
+                using D = Dir<i>;
+                const float wp = D::w * psi[int(id) + D::cx + g.sy * D::cy + g.sz * D::cz];
+                if constexpr (D::cx != 0) sx += D::fx * wp;
+                if constexpr (D::cy != 0) sy += D::fy * wp;
+                if constexpr (D::cz != 0) sz += D::fz * wp;
+            });
+            Fx = kInvCs2 * sx;
+            Fy = kInvCs2 * sy;
+            Fz = kInvCs2 * sz;
+            absF = sqrtf(Fx * Fx + Fy * Fy + Fz * Fz);
+            has_dir = !(absF <= 1.0e-4f);
+            K = ph.beta * ((rr * rb) / (rho * rho)) * rho;
+        }
+        const float invF = has_dir ? 1.0f / absF : 0.0f;
+        float l_aR = 0.f, l_aB = 0.f, l_rhoeq = 0.f, l_uP[3] = {0.f, 0.f, 0.f}, l_uQ = 0.f, l_oms = 0.f;
+        float S2[6] = {0, 0, 0, 0, 0, 0}, S3[7] = {0, 0, 0, 0, 0, 0, 0};
+        float sA[3] = {0, 0, 0}, sB = 0.f, sD[3] = {0, 0, 0}, sE = 0.f, sBB = 0.f, l_Ah = 0.f;
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            using D = Dir<i>;
+            const float lr = lam_load(lam, g, slot_f32(i, 0), x, y, z);
+            const float lb = lam_load(lam, g, slot_f32(i, 1), x, y, z);
+            const float fe = feq<i>(rho, e);
+            const float fn = fneq<i>(n);
+            float cu = 0.f, fc = 0.f;
+            if constexpr (D::cx != 0) { cu += D::fx * ux; fc += D::fx * Fx; }
+            if constexpr (D::cy != 0) { cu += D::fy * uy; fc += D::fy * Fy; }
+            if constexpr (D::cz != 0) { cu += D::fz * uz; fc += D::fz * Fz; }
+            float om2 = 0.f, om2_over_Ah = 0.f, dlt = 0.f;
+            if (interface) {
+                const float cos2 = (i != 0 && has_dir) ? fc * fc * invF * invF : 0.0f;
+                om2_over_Ah = absF * (D::w * cos2 - D::B);
+                om2 = ph.Ah * om2_over_Ah;
+                if (i != 0 && has_dir) dlt = K * D::w * D::invc * fc * invF;
+            }
+            const float gi = fe + oms * fn + om2;
+            l_aR += lr * gi;
+            l_aB += lb * gi;
+            const float lg = aR * lr + aB * lb;
+            const float ld = lr - lb;
+            l_rhoeq += lg * fe;
+            // d feq / d u = w rho [c P - u Q]
+            const float P = kInvCs2 + cu * (2.0f * kInv2Cs4) + (cu * cu) * (3.0f * kInv6Cs6) - e.usq * kInv2Cs4;
+            const float Q = kInvCs2 + cu * (2.0f * kInv2Cs4);
+            const float wl = lg * D::w * rho;
+            if constexpr (D::cx != 0) l_uP[0] += wl * P * D::fx;
+            if constexpr (D::cy != 0) l_uP[1] += wl * P * D::fy;
+            if constexpr (D::cz != 0) l_uP[2] += wl * P * D::fz;
+            l_uQ += wl * Q;
+            l_oms += lg * fn;
+            const float mu = oms * lg * D::w;
+            S2[0] += mu * D::Hxx; S2[1] += mu * D::Hxy; S2[2] += mu * D::Hyy;
+            S2[3] += mu * D::Hyz; S2[4] += mu * D::Hzz; S2[5] += mu * D::Hxz;
+            if constexpr (D::Hxxy != 0.0f) S3[0] += mu * D::Hxxy;
+            if constexpr (D::Hxxz != 0.0f) S3[1] += mu * D::Hxxz;
+            if constexpr (D::Hxyy != 0.0f) S3[2] += mu * D::Hxyy;
+            if constexpr (D::Hxzz != 0.0f) S3[3] += mu * D::Hxzz;
+            if constexpr (D::Hyyz != 0.0f) S3[4] += mu * D::Hyyz;
+            if constexpr (D::Hyzz != 0.0f) S3[5] += mu * D::Hyzz;
+            if constexpr (D::Hxyz != 0.0f) S3[6] += mu * D::Hxyz;
+            if (interface) {
+                sBB += lg * D::B;
+                l_Ah += lg * om2_over_Ah;
+                if (i != 0 && has_dir) {
+                    const float a = lg * D::w * fc, d = ld * D::w * D::invc;
+                    if constexpr (D::cx != 0) { sA[0] += a * D::fx; sD[0] += d * D::fx; }
+                    if constexpr (D::cy != 0) { sA[1] += a * D::fy; sD[1] += d * D::fy; }
+                    if constexpr (D::cz != 0) { sA[2] += a * D::fz; sD[2] += d * D::fz; }
+                    sB += lg * D::w * fc * fc;
+                    sE += d * fc;
+                }
+            }
+        });
+        // fneq: Pi enters directly (H2) and through the third-order terms a3
+        const float c2 = kInv2Cs4, c3 = kInv2Cs6;
+        float lPxx = S2[0] * c2, lPxy = 2.0f * S2[1] * c2, lPyy = S2[2] * c2;
+        float lPyz = 2.0f * S2[3] * c2, lPzz = S2[4] * c2, lPxz = 2.0f * S2[5] * c2;
+        const float la_xxy = S3[0] * c3, la_xxz = S3[1] * c3, la_xyy = S3[2] * c3, la_xzz = S3[3] * c3;
+        const float la_yyz = S3[4] * c3, la_yzz = S3[5] * c3, la_xyz = 2.0f * S3[6] * c3;
+        float lux = 0.f, luy = 0.f, luz = 0.f;
+        lPxx += la_xxy * uy + la_xxz * uz;
+        lPyy += la_xyy * ux + la_yyz * uz;
+        lPzz += la_xzz * ux + la_yzz * uy;
+        lPxy += 2.0f * la_xxy * ux + 2.0f * la_xyy * uy + la_xyz * uz;
+        lPxz += 2.0f * la_xxz * ux + 2.0f * la_xzz * uz + la_xyz * uy;
+        lPyz += 2.0f * la_yyz * uy + 2.0f * la_yzz * uz + la_xyz * ux;
+        lux += 2.0f * la_xxy * n.pxy + 2.0f * la_xxz * n.pxz + la_xyy * n.pyy + la_xzz * n.pzz + la_xyz * n.pyz;
+        luy += la_xxy * n.pxx + 2.0f * la_xyy * n.pxy + 2.0f * la_yyz * n.pyz + la_yzz * n.pzz + la_xyz * n.pxz;
+        luz += la_xxz * n.pxx + 2.0f * la_xzz * n.pxz + la_yyz * n.pyy + 2.0f * la_yzz * n.pyz + la_xyz * n.pxy;
+        // feq
+        lux += l_uP[0] - ux * l_uQ;
+        luy += l_uP[1] - uy * l_uQ;
+        luz += l_uP[2] - uz * l_uQ;
+        // colour gradient: perturbation and recolouring
+        float lFx = 0.f, lFy = 0.f, lFz = 0.f, lK = 0.f;
+        if (interface) {
+            const float ah = ph.Ah;
+            if (has_dir) {
+                const float i3 = invF * invF * invF;
+                lFx = ah * (2.0f * invF * sA[0] - Fx * i3 * sB - Fx * invF * sBB) + K * (sD[0] * invF - Fx * i3 * sE);
+                lFy = ah * (2.0f * invF * sA[1] - Fy * i3 * sB - Fy * invF * sBB) + K * (sD[1] * invF - Fy * i3 * sE);
+                lFz = ah * (2.0f * invF * sA[2] - Fz * i3 * sB - Fz * invF * sBB) + K * (sD[2] * invF - Fz * i3 * sE);
+                lK = sE * invF;
+            } else if (absF > 0.0f) {
+                const float q = -ah * sBB / absF;
+                lFx = q * Fx;
+                lFy = q * Fy;
+                lFz = q * Fz;
+            }
+        }
+        const float inv2 = invr * invr;
+        const float l_rho = l_rhoeq * invr;  // feq is proportional to rho
+        const float lrr = l_rho + (l_aR - l_aB) * rb * inv2 + lK * ph.beta * rb * rb * inv2;
+        const float lrb = l_rho - (l_aR - l_aB) * rr * inv2 + lK * ph.beta * rr * rr * inv2;
+        lmom[kMomRR * N + id] = lrr;
+        lmom[kMomRB * N + id] = lrb;
+        lmom[kMomUX * N + id] = lux;
+        lmom[kMomUY * N + id] = luy;
+        lmom[kMomUZ * N + id] = luz;
+        lmom[kMomPXX * N + id] = lPxx;
+        lmom[kMomPXY * N + id] = lPxy;
+        lmom[kMomPYY * N + id] = lPyy;
+        lmom[kMomPYZ * N + id] = lPyz;
+        lmom[kMomPZZ * N + id] = lPzz;
+        lmom[kMomPXZ * N + id] = lPxz;
+        lf[0 * N + id] = lFx;
+        lf[1 * N + id] = lFy;
+        lf[2 * N + id] = lFz;
+        a_omega = -double(l_oms);  // oms = 1 - omega
+        a_Ah = double(l_Ah);
+    }
+    const double r0 = block_sum_any(a_omega, sh, kBX * kBY);
+    const double r1 = block_sum_any(a_Ah, sh, kBX * kBY);
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        atomicAdd(acc, r0);
+        atomicAdd(acc + 1, r1);
+    }
+}
+
+// Per node: the psi-adjoint gathered from the neighbours' F-adjoints, then back
+// through the moments to the 54 pulled populations, stored at their pull
+// sources (transposed streaming) in lam_out.
+__global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *lmom, const float *lf,
+                                                          float *lam_out) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
+    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+    const size_t N = g.N;
+    const float *mom = s.mom;
+    const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
+    const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
+    const float rho = rr + rb;
+    // psi(y) enters F(y - c_j) with weight w_j c_j / cs2 (periodic neighbours)
+    float lpsi = 0.f;
+    static_for<kQ - 1>([&](auto I) {
+        constexpr int i = decltype(I)::value + 1;
+        using D = Dir<i>;
+        const int xn = wrap_interior(x - D::cx, g.NX), yn = wrap_interior(y - D::cy, g.NY),
+                  zn = wrap_interior(z - D::cz, g.NZ);
+        const uint32_t nid = uint32_t(xn) + uint32_t(g.sy) * uint32_t(yn) + uint32_t(g.sz) * uint32_t(zn);
+        float dot = 0.f;
+        if constexpr (D::cx != 0) dot += D::fx * lf[0 * N + nid];
+        if constexpr (D::cy != 0) dot += D::fy * lf[1 * N + nid];
+        if constexpr (D::cz != 0) dot += D::fz * lf[2 * N + nid];
+        lpsi += D::w * dot;
+    });
+    lpsi *= kInvCs2;
+    const float inv2 = 1.0f / (rho * rho);
+    const float lrr = lmom[kMomRR * N + id] + lpsi * 2.0f * rb * inv2;
+    const float lrb = lmom[kMomRB * N + id] - lpsi * 2.0f * rr * inv2;
+    const float lPxx = lmom[kMomPXX * N + id], lPxy = lmom[kMomPXY * N + id], lPyy = lmom[kMomPYY * N + id];
+    const float lPyz = lmom[kMomPYZ * N + id], lPzz = lmom[kMomPZZ * N + id], lPxz = lmom[kMomPXZ * N + id];
+    // Pi = A - rho u u
+    const float lux = lmom[kMomUX * N + id] - rho * (2.0f * ux * lPxx + uy * lPxy + uz * lPxz);
+    const float luy = lmom[kMomUY * N + id] - rho * (2.0f * uy * lPyy + ux * lPxy + uz * lPyz);
+    const float luz = lmom[kMomUZ * N + id] - rho * (2.0f * uz * lPzz + ux * lPxz + uy * lPyz);
+    float lrho = -(lPxx * ux * ux + lPxy * ux * uy + lPyy * uy * uy + lPyz * uy * uz + lPzz * uz * uz + lPxz * ux * uz);
+    // u = j / rho
+    const float invr = 1.0f / rho;
+    const float ljx = lux * invr, ljy = luy * invr, ljz = luz * invr;
+    lrho -= (lux * ux + luy * uy + luz * uz) * invr;
+    const PullMap<CodecF32> pm(g, x, y, z, true);
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        using D = Dir<i>;
+        float lgi = lPxx * D::Hxx + lPyy * D::Hyy + lPzz * D::Hzz;
+        if constexpr (D::Hxy != 0.0f) lgi += lPxy * D::Hxy;
+        if constexpr (D::Hyz != 0.0f) lgi += lPyz * D::Hyz;
+        if constexpr (D::Hxz != 0.0f) lgi += lPxz * D::Hxz;
+        if constexpr (D::cx != 0) lgi += D::fx * ljx;
+        if constexpr (D::cy != 0) lgi += D::fy * ljy;
+        if constexpr (D::cz != 0) lgi += D::fz * ljz;
+        lgi += lrho;
+        size_t grow;
+        int xs;
+        pm.template src<i>(x, grow, xs);
+        lam_out[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrr + lgi;
+        lam_out[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrb + lgi;
+    });
+}
+
+// dJ/du0 for an initial state f0_c,i = feq_i(rho_c, u0): pulls lambda_0 like
+// the forward step pulls populations.
+__global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, const float *lam0, float *du0) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z = blockIdx.z;
+    if (x >= g.NX || y >= g.NY) return;
+    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
+    const size_t N = g.N;
+    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) {
+        du0[id] = du0[N + id] = du0[2 * N + id] = 0.0f;
+        return;
+    }
+    const float *mom = s.mom;
+    const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
+    const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
+    const EqTerms e = make_eq(ux, uy, uz);
+    const PullMap<CodecF32> pm(g, x, y, z, true);
+    float gx = 0.f, gy = 0.f, gz = 0.f, gq = 0.f;
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        using D = Dir<i>;
+        size_t grow;
+        int xs;
+        pm.template src<i>(x, grow, xs);
+        const float lr = lam0[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs];
+        const float lb = lam0[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs];
+        float cu = 0.f;
+        if constexpr (D::cx != 0) cu += D::fx * ux;
+        if constexpr (D::cy != 0) cu += D::fy * uy;
+        if constexpr (D::cz != 0) cu += D::fz * uz;
+        const float P = kInvCs2 + cu * (2.0f * kInv2Cs4) + (cu * cu) * (3.0f * kInv6Cs6) - e.usq * kInv2Cs4;
+        const float Q = kInvCs2 + cu * (2.0f * kInv2Cs4);
+        const float wl = D::w * (lr * rr + lb * rb);
+        if constexpr (D::cx != 0) gx += wl * P * D::fx;
+        if constexpr (D::cy != 0) gy += wl * P * D::fy;
+        if constexpr (D::cz != 0) gz += wl * P * D::fz;
+        gq += wl * Q;
+    });
+    du0[id] = gx - ux * gq;
+    du0[N + id] = gy - uy * gq;
+    du0[2 * N + id] = gz - uz * gq;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------- host side
@@ -1180,6 +1540,25 @@ cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaSt
     if (e != cudaSuccess) return e;
     if (s.g.storage == kStoreF16) k_check_finite<CodecF16><<<grid1(s.g), kRedThreads, 0, st>>>(s, cur, flag);
     else k_check_finite<CodecF32><<<grid1(s.g), kRedThreads, 0, st>>>(s, cur, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_terminal(const DeviceState &s, const float *target, float *lam, double *J, cudaStream_t st) {
+    k_adj_terminal<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, target, lam, J);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_step(const DeviceState &s, int64_t step, const float *lam_in, float *lmom, float *lf,
+                            float *lam_out, double *acc, cudaStream_t st) {
+    k_adj_collide<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, step, lam_in, lmom, lf, acc);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_adj_moments<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, lmom, lf, lam_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_initial(const DeviceState &s, const float *lam0, float *du0, cudaStream_t st) {
+    k_adj_initial<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, lam0, du0);
     return cudaGetLastError();
 }
 

@@ -113,7 +113,8 @@ cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int wh
 cudaError_t launch_accumulate_radial(const DeviceState &s, cudaStream_t st);
 
 // Initial state.  mode 0: jet (jet/jetIn.cuh), 1: bubble (bubble/bubbleIn.cuh),
-// 2: populations from reference-layout device arrays fr_ref/fb_ref.
+// 2: populations from reference-layout device arrays fr_ref/fb_ref,
+// 3: per-colour equilibrium feq(rho_c, u) of the moment planes rr, rb, u.
 cudaError_t launch_init_fields(const DeviceState &s, int mode, int red_inside, float bubble_r2, float bx, float by,
                                float bz, cudaStream_t st);
 cudaError_t launch_init_pops(const DeviceState &s, int mode, const float *fr_ref, const float *fb_ref, float noise,
@@ -131,5 +132,16 @@ cudaError_t launch_uy_average(const DeviceState &s, uint32_t samples, cudaStream
 uint32_t conservation_blocks(const Geometry &g);
 cudaError_t launch_conservation(const DeviceState &s, int cur, double *partials, double *out5, cudaStream_t st);
 cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaStream_t st);
+
+// ---- discrete adjoint of the step (periodic box, float32 populations) ----
+// lambda buffers share the population layout.  Terminal condition for
+// J = sum (psi_T - target)^2 (needs the moment planes of S_T), one adjoint step
+// (needs the moment planes and psi of S_t; lmom [11][N], lf [3][N] scratch;
+// acc[0] += dJ/domega, acc[1] += dJ/d(A/2)), and dJ/du0 of a state
+// f0 = feq(rho_c, u0) (needs the moment planes of S_0; du0 [3][N]).
+cudaError_t launch_adj_terminal(const DeviceState &s, const float *target, float *lam, double *J, cudaStream_t st);
+cudaError_t launch_adj_step(const DeviceState &s, int64_t step, const float *lam_in, float *lmom, float *lf,
+                            float *lam_out, double *acc, cudaStream_t st);
+cudaError_t launch_adj_initial(const DeviceState &s, const float *lam0, float *du0, cudaStream_t st);
 
 }  // namespace mcg

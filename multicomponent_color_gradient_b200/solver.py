@@ -107,6 +107,28 @@ class Solver:
 
     init_bubble = launch_bubble
 
+    def init_equilibrium(self, rhor, rhob, ux, uy, uz) -> None:
+        """Per-colour equilibrium feq(rho_c, u) at every interior node (the
+        bubble and jet initial states are the u = 0 case)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32).reshape(-1) for a in (rhor, rhob, ux, uy, uz)]
+        assert all(a.size == self.N for a in arrs)
+        self._c("mcg_init_equilibrium", *[_fptr(a) for a in arrs])
+
+    # -- discrete adjoint (periodic box, float32 storage) ----------------------
+    def adjoint_run(self, psi_target, nsteps: int, snapshots: int) -> Dict:
+        """J = sum (psi_T - psi_target)^2 over interior nodes after `nsteps`
+        steps from the current state, with dJ/dsigma, dJ/dtau and dJ/du0
+        ((3, Ncells) float32) from one reverse sweep; the state is unchanged."""
+        tgt = np.ascontiguousarray(psi_target, dtype=np.float32).reshape(-1)
+        assert tgt.size == self.N
+        J, ds, dt = C.c_double(), C.c_double(), C.c_double()
+        du0 = np.empty(3 * self.N, np.float32)
+        fwd, ms = C.c_int64(), C.c_float()
+        self._c("mcg_adjoint_run", _fptr(tgt), int(nsteps), int(snapshots), C.byref(J), C.byref(ds), C.byref(dt),
+                _fptr(du0), C.byref(fwd), C.byref(ms))
+        return {"J": J.value, "dJ_dsigma": ds.value, "dJ_dtau": dt.value, "dJ_du0": du0.reshape(3, self.N),
+                "forward_steps": int(fwd.value), "ms": float(ms.value)}
+
     # -- the per-step sequence (main.cu:52-82) -------------------------------
     def launch_Macros(self) -> None:
         self._c("mcg_macros")
@@ -252,6 +274,14 @@ class Solver:
 
     def output_close(self) -> None:
         self._c("mcg_output_close")
+
+
+def adjoint_plan(nsteps: int, snapshots: int):
+    """(forward steps, recomputation depth r) of the checkpointing schedule."""
+    lib = _lib.load()
+    f, r = C.c_int64(), C.c_int32()
+    _lib.check(lib.mcg_adjoint_plan(int(nsteps), int(snapshots), C.byref(f), C.byref(r)), "mcg_adjoint_plan")
+    return int(f.value), int(r.value)
 
 
 def device_count() -> int:

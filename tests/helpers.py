@@ -113,3 +113,16 @@ def psi_of(rr, rb):
     rr = np.asarray(rr, np.float64)
     rb = np.asarray(rb, np.float64)
     return (rr - rb) / (rr + rb)
+
+
+def feq64(rho, ux, uy, uz):
+    """Third-order Hermite equilibrium (lbm.cuh:16-35) in float64, reference
+    layout (Q, Ncells)."""
+    w = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8, np.float64)
+    cs2 = 1.0 / 3.0
+    rho, ux, uy, uz = (np.asarray(a, np.float64) for a in (rho, ux, uy, uz))
+    cu = CX[:, None] * ux[None, :] + CY[:, None] * uy[None, :] + CZ[:, None] * uz[None, :]
+    usq = (ux * ux + uy * uy + uz * uz)[None, :]
+    a2 = cu * cu / (2 * cs2 * cs2) - usq / (2 * cs2) + cu / cs2
+    a3 = cu * (cu * cu / (6 * cs2 ** 3) - usq / (2 * cs2 * cs2))
+    return w[:, None] * rho[None, :] * (1.0 + a2 + a3)

@@ -1,0 +1,69 @@
+"""Host-side pieces of the discrete adjoint (no GPU): the binomial
+checkpointing schedule and the Fourier-mode parametrisation of u0."""
+import functools
+
+import numpy as np
+import pytest
+
+from multicomponent_color_gradient_b200 import get_case
+from multicomponent_color_gradient_b200.adjoint import FourierModes
+from multicomponent_color_gradient_b200.solver import adjoint_plan
+
+
+@functools.lru_cache(maxsize=None)
+def optimal_forward_steps(n, s):
+    """Fewest forward steps that reverse n ops (op t needs state t) holding the
+    first state plus s free slots: exhaustive over every split point."""
+    if n == 1:
+        return 0
+    if s == 0:
+        return n * (n - 1) // 2
+    return min(m + optimal_forward_steps(n - m, s - 1) + optimal_forward_steps(m, s) for m in range(1, n))
+
+
+@pytest.mark.parametrize("snapshots", [1, 2, 3, 4, 6])
+def test_schedule_is_optimal(snapshots):
+    for T in range(1, 41):
+        fwd, r = adjoint_plan(T, snapshots)
+        s = min(snapshots - 1, T)
+        assert fwd == optimal_forward_steps(T + 1, s), (T, snapshots, fwd)
+
+
+def test_schedule_with_a_slot_per_state_runs_each_step_once():
+    for T in (1, 7, 100, 1000):
+        assert adjoint_plan(T, T + 1) == (T, 1)
+        assert adjoint_plan(T, T + 50) == (T, 1)
+        assert adjoint_plan(T, 1) == (T * (T + 1) // 2, T)
+
+
+def test_schedule_depth_is_binomial():
+    # r least with C(s + r, s) >= T + 1 (s = snapshots - 1)
+    from math import comb
+    for T, snaps in ((1000, 4), (500, 10), (64, 2)):
+        f, r = adjoint_plan(T, snaps)
+        assert comb(snaps + r, snaps) >= T + 1 > comb(snaps + r - 1, snaps)
+        # Griewank's minimum: r n - C(s + r, s + 1) forward steps for n = T + 1 ops
+        assert f == r * (T + 1) - comb(snaps + r, snaps + 1)
+
+
+def test_fourier_modes_are_divergence_free_and_project_is_the_transpose():
+    case = get_case("adjoint_bubble_96", NX=14, NY=12, NZ=10)
+    M = FourierModes(case, max_mode=1, seed=5)
+    assert M.count == 26
+    assert np.allclose(np.einsum("mc,mc->m", M.k, M.e), 0.0)
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=M.count)
+    v = rng.normal(size=(3, M.N))
+    lhs = float(np.sum(M.velocity(a) * v))
+    rhs = float(a @ M.project(v))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
+    u = M.velocity(a).reshape(3, 10, 12, 14)
+    assert np.all(u[:, 0] == 0) and np.all(u[:, :, :, -1] == 0)
+    # periodic over the interior: the field at x = 1 continues the one at x = NX - 2
+    ux = u[0, 1:-1, 1:-1, 1:-1]
+    L = 12
+    xi = np.arange(L + 1)
+    k = M.k[:, 0]
+    val = np.cos(np.outer(xi, k) + M.phase[None, :]) @ (a * M.e[:, 0])
+    assert np.allclose(val[0], val[L])
+    assert np.allclose(ux[0, 0, :], val[:L])
