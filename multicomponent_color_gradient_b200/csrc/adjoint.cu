@@ -14,10 +14,16 @@
 // of splits that reach the fewest forward steps, r n - beta(s + 1, r - 1).
 // With s >= n every state is made once (T forward steps).
 //
-// Snapshots are full population buffers in HBM.  Forward steps write straight
-// into the next slot (or ping-pong through two work buffers for longer
-// segments), so no state is ever copied.  The run's moment planes and colour
-// fields live in their own buffers: the handle's state is left untouched.
+// An op reads its state only through the state's moment record (11 moment
+// planes and psi, 48 B per node).  With a slot for every state (snapshots >
+// nsteps) the sweep keeps no populations at all: one forward pass in which the
+// fused step records each state's moments as it pulls them (a tape of
+// (T + 1) records), then T + 1 ops.  With fewer slots the slots hold
+// population buffers (216 B per node) as restart points, forward steps write
+// straight into the next slot (or ping-pong through two work buffers for longer
+// segments) so no state is ever copied, and each op first forms its record
+// with the moments kernel.  The run's records live in their own buffers: the
+// handle's state is left untouched.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -119,6 +125,7 @@ struct DeviceBuffers {
 struct Run {
     mcg_handle *h = nullptr;
     mcg::DeviceState base{};   // the handle's state with the run's own moment / psi planes
+    float *rec = nullptr;      // moment record of the op's state (checkpoint mode)
     std::vector<void *> slots; // slots[0] = S_0 (the handle's buffer)
     void *work[2] = {nullptr, nullptr};
     float *lam[2] = {nullptr, nullptr};
@@ -149,18 +156,44 @@ struct Run {
         return MCG_OK;
     }
 
-    // op t on the state held in `state`
-    mcg_status op(void *state, int64_t t) {
-        const mcg::DeviceState d = with(state, nullptr);
-        ADJ_LAUNCH(h, mcg::launch_moments(d, 0, step0 + t, false, h->stream), "adjoint: moments");
+    // op t with the moment record M of S_t
+    mcg_status op_record(const float *M, int64_t t) {
         if (t == T) {
-            ADJ_LAUNCH(h, mcg::launch_adj_terminal(d, target, lam[lc], acc, h->stream), "adjoint: terminal");
+            ADJ_LAUNCH(h, mcg::launch_adj_terminal(base, M, target, lam[lc], acc, h->stream), "adjoint: terminal");
         } else {
-            ADJ_LAUNCH(h, mcg::launch_adj_step(d, step0 + t, lam[lc], lmom, lf, lam[lc ^ 1], acc + 1, h->stream),
+            ADJ_LAUNCH(h, mcg::launch_adj_step(base, M, lam[lc], lmom, lf, lam[lc ^ 1], acc + 1, h->stream),
                        "adjoint: step");
             h->launches += 1;  // two kernels
             lc ^= 1;
         }
+        return MCG_OK;
+    }
+
+    // op t on the state held in `state` (its record formed first)
+    mcg_status op(void *state, int64_t t) {
+        ADJ_LAUNCH(h, mcg::launch_moments(with(state, nullptr), 0, step0 + t, false, h->stream), "adjoint: moments");
+        return op_record(rec, t);
+    }
+
+    // Tape mode: one forward pass recording every state's moments into
+    // tape[t] (t < T by the fused steps, T by the moments kernel), then the ops.
+    mcg_status run_tape(float *tape, size_t record_floats) {
+        void *a = slots[0];
+        for (int64_t t = 0; t < T; ++t) {
+            mcg::DeviceState d = with(a, work[t & 1]);
+            d.tape = tape + size_t(t) * record_floats;
+            ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "adjoint: forward step");
+            a = work[t & 1];
+        }
+        {
+            mcg::DeviceState d = with(a, nullptr);
+            float *M = tape + size_t(T) * record_floats;
+            d.mom = M;
+            d.psi[0] = d.psi[1] = M + size_t(mcg::kTapePsi) * base.g.N;
+            ADJ_LAUNCH(h, mcg::launch_moments(d, 0, step0 + T, false, h->stream), "adjoint: moments");
+        }
+        for (int64_t t = T; t >= 0; --t)
+            if (mcg_status s = op_record(tape + size_t(t) * record_floats, t)) return s;
         return MCG_OK;
     }
 
@@ -206,10 +239,12 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
     const mcg::Geometry &g = h->s.g;
     const size_t N = g.N;
     const size_t pop_bytes = size_t(g.slots) * N * sizeof(float);
-    const int free_slots = int(std::min<int64_t>(snapshots - 1, nsteps));
+    const size_t record_floats = size_t(mcg::kTapePlanes) * N;
+    const bool tape_mode = snapshots > nsteps;
+    const int free_slots = tape_mode ? 0 : snapshots - 1;
 
     std::vector<Action> acts;
-    plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
+    if (!tape_mode) plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
 
     DeviceBuffers buf;
     Run run;
@@ -230,11 +265,16 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
         ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint lambda buffers");
         run.lam[k] = static_cast<float *>(p);
     }
-    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment planes");
-    run.base.mom = static_cast<float *>(p);
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "adjoint psi planes");
-        run.base.psi[k] = static_cast<float *>(p);
+    float *tape = nullptr;
+    if (tape_mode) {
+        ADJ_CUDA(buf.alloc(&p, (size_t(nsteps) + 1) * record_floats * sizeof(float)), "adjoint moment tape");
+        tape = static_cast<float *>(p);
+    } else {
+        ADJ_CUDA(buf.alloc(&p, record_floats * sizeof(float)), "adjoint moment record");
+        run.rec = static_cast<float *>(p);
+        // the moments kernel writes the record: 11 planes, then psi (ghost mirrors unused)
+        run.base.mom = run.rec;
+        run.base.psi[0] = run.base.psi[1] = run.rec + size_t(mcg::kTapePsi) * N;
     }
     ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment adjoints");
     run.lmom = static_cast<float *>(p);
@@ -249,9 +289,14 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
     run.acc = static_cast<double *>(p);
 
     ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
-    if (mcg_status s = run.execute(acts)) return s;
-    // op 0 left the moments of S_0 in the run's planes
-    ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
+    if (tape_mode) {
+        if (mcg_status s = run.run_tape(tape, record_floats)) return s;
+    } else {
+        if (mcg_status s = run.execute(acts)) return s;
+    }
+    // op 0 was the last: its record is S_0's
+    const float *M0 = tape_mode ? tape : run.rec;
+    ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, M0, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
     ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
     double acc[3] = {0, 0, 0};
     ADJ_CUDA(cudaMemcpyAsync(acc, run.acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream), "download J");
@@ -269,7 +314,7 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
     if (J) *J = acc[0];
     if (dJ_dsigma) *dJ_dsigma = acc[2] * dAh_dsigma;
     if (dJ_dtau) *dJ_dtau = acc[1] * (-omega * omega) + acc[2] * (-Ah / tau);
-    if (forward_steps) *forward_steps = forward_steps_of(acts);
+    if (forward_steps) *forward_steps = tape_mode ? int64_t(nsteps) : forward_steps_of(acts);
     if (ms) *ms = t_ms;
     return MCG_OK;
 }

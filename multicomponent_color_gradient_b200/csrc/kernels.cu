@@ -26,6 +26,7 @@
 // inlet columns, y=NY-2 slots fed by ghost columns) are ghost-plane values of
 // both buffers that no kernel writes, so results are the same.
 #include <cooperative_groups.h>
+#include <type_traits>
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -499,6 +500,15 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
                                                     m.pyz, m.pzz, m.pxz};
 #pragma unroll
                         for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
+                    }
+                    if (std::is_same<C, CodecF32>::value && kPeriodic && s.tape) {
+                        // moment record of the pulled state (the adjoint sweep reads it)
+                        float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
+                        const size_t N = g.N;
+                        const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy,
+                                                      m.pyz, m.pzz, m.pxz, ps};
+#pragma unroll
+                        for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
                     }
                 }
             }
@@ -1056,6 +1066,10 @@ cudaError_t boundary_dispatch(const DeviceState &s, int wbuf, int64_t step, int 
 // transposed streaming.  The bulk/interface switch (I <= 1e-4) and the
 // |F| <= 1e-4 cut-off are taken as in the forward step (derivatives inside
 // the branch the forward state selects).
+//
+// Every pass reads the state S_t only through its moment record M: the 11
+// moment planes of the pulled populations and psi (plane kTapePsi), interior
+// nodes; neighbours are addressed with the periodic wrap.
 
 __device__ __forceinline__ double block_sum_any(double v, double *sh, int nthreads) {
 #pragma unroll
@@ -1072,13 +1086,9 @@ __device__ __forceinline__ double block_sum_any(double v, double *sh, int nthrea
     return r;
 }
 
-__device__ __forceinline__ float lam_load(const float *lam, const Geometry &g, int slot, int x, int y, int z) {
-    return lam[pop_index(g, slot, x, y, z)];
-}
-
 // J = sum over interior nodes of (psi_T - psi*)^2 and lambda_T = dJ/dS_T.
-__global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s, const float *__restrict__ target,
-                                                           float *lam, double *J) {
+__global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s, const float *__restrict__ M,
+                                                           const float *__restrict__ target, float *lam, double *J) {
     __shared__ double sh[kBX * kBY / 32];
     const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
@@ -1089,9 +1099,9 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
     if (in) {
         const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
         const size_t N = g.N;
-        const float rr = s.mom[kMomRR * N + id], rb = s.mom[kMomRB * N + id];
+        const float rr = M[kMomRR * N + id], rb = M[kMomRB * N + id];
         const float rho = rr + rb;
-        const float d = (rr - rb) / rho - target[id];
+        const float d = M[kTapePsi * N + id] - target[id];
         jloc = double(d) * double(d);
         const float lpsi = 2.0f * d;
         const float inv2 = 1.0f / (rho * rho);
@@ -1113,8 +1123,18 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
 // Per node: lambda_post (54 values at the node) -> adjoints of the node's
 // moments (11, to lmom) and colour gradient (3, to lf); float64 partials of
 // dJ/domega (acc[0]) and dJ/d(A/2) (acc[1]).
-__global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, int64_t step, const float *lam,
-                                                          float *lmom, float *lf, double *acc) {
+//
+// Per direction the stored pair is r_i = aR g_i + D_i, b_i = aB g_i - D_i, so
+// with lg_i = aR lr_i + aB lb_i and ld_i = lr_i - lb_i the node's sums are
+//   d/d(aR - aB)-part  sum ld_i g_i,   d/drho  sum lg_i feq_i / rho,
+//   d/du     sum lg_i w rho (c P_i - u Q_i)  (dfeq/du),
+//   d/dPi    oms sum lg_i w H2_i / 2cs4 and the third-order a3 chain,
+//   d/domega -sum lg_i fneq_i,  d/dF from Omega2 and D,  d/dK from D.
+// Opposite directions i, i+1 are taken together: feq and fneq split into even
+// and odd parts, Omega2 is even and D odd, so every sum needs only
+// lg_i + lg_o, lg_i - lg_o, ld_i + ld_o and ld_i - ld_o.
+__global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState s, const float *__restrict__ M,
+                                                             const float *lam, float *lmom, float *lf, double *acc) {
     __shared__ double sh[kBX * kBY / 32];
     const Geometry &g = s.g;
     const Physics &ph = s.ph;
@@ -1126,12 +1146,12 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, 
     if (in) {
         const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
         const size_t N = g.N;
-        const float *mom = s.mom;
+        const float *mom = M;
         const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
         const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
         const NeqTerms n = make_neq(mom[kMomPXX * N + id], mom[kMomPXY * N + id], mom[kMomPYY * N + id],
                                     mom[kMomPYZ * N + id], mom[kMomPZZ * N + id], mom[kMomPXZ * N + id], ux, uy, uz);
-        const EqTerms e = make_eq(ux, uy, uz);
+        const float usq = ux * ux + uy * uy + uz * uz;
         const float rho = rr + rb;
         const float invr = 1.0f / rho;
         const float aR = rr * invr, aB = rb * invr;
@@ -1140,12 +1160,15 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, 
         float Fx = 0.f, Fy = 0.f, Fz = 0.f, absF = 0.f, K = 0.f;
         bool has_dir = false;
         if (interface) {
-            const float *psi = s.psi[step & 1];
+            const float *psi = M + size_t(kTapePsi) * N;
+            const int xn[3] = {wrap_interior(x - 1, g.NX), x, wrap_interior(x + 1, g.NX)};
+            const int yn[3] = {g.sy * wrap_interior(y - 1, g.NY), g.sy * y, g.sy * wrap_interior(y + 1, g.NY)};
+            const int zn[3] = {g.sz * wrap_interior(z - 1, g.NZ), g.sz * z, g.sz * wrap_interior(z + 1, g.NZ)};
             float sx = 0.f, sy = 0.f, sz = 0.f;
             static_for<kQ - 1>([&](auto I) {
                 constexpr int i = decltype(I)::value + 1;
                 using D = Dir<i>;
-                const float wp = D::w * psi[int(id) + D::cx + g.sy * D::cy + g.sz * D::cz];
+                const float wp = D::w * psi[xn[D::cx + 1] + yn[D::cy + 1] + zn[D::cz + 1]];
                 if constexpr (D::cx != 0) sx += D::fx * wp;
                 if constexpr (D::cy != 0) sy += D::fy * wp;
                 if constexpr (D::cz != 0) sz += D::fz * wp;
@@ -1158,97 +1181,132 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, 
             K = ph.beta * ((rr * rb) / (rho * rho)) * rho;
         }
         const float invF = has_dir ? 1.0f / absF : 0.0f;
-        float l_aR = 0.f, l_aB = 0.f, l_rhoeq = 0.f, l_uP[3] = {0.f, 0.f, 0.f}, l_uQ = 0.f, l_oms = 0.f;
+        const float invF2 = invF * invF;
+        const float Ah = ph.Ah;
+        float l_d = 0.f, l_rhoeq = 0.f, l_uPx = 0.f, l_uPy = 0.f, l_uPz = 0.f, l_uQ = 0.f, l_oms = 0.f;
         float S2[6] = {0, 0, 0, 0, 0, 0}, S3[7] = {0, 0, 0, 0, 0, 0, 0};
-        float sA[3] = {0, 0, 0}, sB = 0.f, sD[3] = {0, 0, 0}, sE = 0.f, sBB = 0.f, l_Ah = 0.f;
-        static_for<kQ>([&](auto I) {
-            constexpr int i = decltype(I)::value;
+        float sAx = 0.f, sAy = 0.f, sAz = 0.f, sB = 0.f, sDx = 0.f, sDy = 0.f, sDz = 0.f, sE = 0.f, sBB = 0.f,
+              l_Ah = 0.f;
+        const size_t row = pop_row(g, y, z);
+        auto lam_at = [&](int slot) { return lam[row + size_t(slot) * size_t(g.NX) + size_t(x)]; };
+        {  // rest direction: even only
+            const float lr = lam_at(slot_f32(0, 0)), lb = lam_at(slot_f32(0, 1));
+            const float lg = aR * lr + aB * lb, ld = lr - lb;
+            const float w = Dir<0>::w;
+            const float E = 1.0f - usq * kInv2Cs2;
+            const float fe = w * rho * E;
+            const float fn = fneq<0>(n);
+            const float o2A = -absF * Dir<0>::B;  // Omega2 / (A/2)
+            const float ge = fe + oms * fn + (interface ? Ah * o2A : 0.0f);
+            l_d += ld * ge;
+            l_rhoeq += lg * fe;
+            l_uQ += lg * w * rho * kInvCs2;
+            l_oms += lg * fn;
+            const float mu = lg * w;
+            S2[0] += mu * Dir<0>::Hxx;
+            S2[2] += mu * Dir<0>::Hyy;
+            S2[4] += mu * Dir<0>::Hzz;
+            if (interface) {
+                sBB += lg * Dir<0>::B;
+                l_Ah += lg * o2A;
+            }
+        }
+        static_for<(kQ - 1) / 2>([&](auto P) {
+            constexpr int i = 2 * decltype(P)::value + 1;
             using D = Dir<i>;
-            const float lr = lam_load(lam, g, slot_f32(i, 0), x, y, z);
-            const float lb = lam_load(lam, g, slot_f32(i, 1), x, y, z);
-            const float fe = feq<i>(rho, e);
-            const float fn = fneq<i>(n);
+            const float lri = lam_at(slot_f32(i, 0)), lbi = lam_at(slot_f32(i, 1));
+            const float lro = lam_at(slot_f32(i + 1, 0)), lbo = lam_at(slot_f32(i + 1, 1));
+            const float lgi = aR * lri + aB * lbi, lgo = aR * lro + aB * lbo;
+            const float ldi = lri - lbi, ldo = lro - lbo;
+            const float gs = lgi + lgo, gd = lgi - lgo, ds = ldi + ldo, dd = ldi - ldo;
             float cu = 0.f, fc = 0.f;
             if constexpr (D::cx != 0) { cu += D::fx * ux; fc += D::fx * Fx; }
             if constexpr (D::cy != 0) { cu += D::fy * uy; fc += D::fy * Fy; }
             if constexpr (D::cz != 0) { cu += D::fz * uz; fc += D::fz * Fz; }
-            float om2 = 0.f, om2_over_Ah = 0.f, dlt = 0.f;
+            const float wr = D::w * rho;
+            // feq_i = w rho (E + O), feq_o = w rho (E - O)
+            const float E = 1.0f + ((cu * cu) * kInv2Cs4 - usq * kInv2Cs2);
+            const float O = cu * kInvCs2 + cu * ((cu * cu) * kInv6Cs6 - usq * kInv2Cs4);
+            // fneq_i = w (A2 + A3), fneq_o = w (A2 - A3)
+            const float A2 = (n.pxx * D::Hxx + 2.0f * n.pxy * D::Hxy + n.pyy * D::Hyy + 2.0f * n.pyz * D::Hyz +
+                              n.pzz * D::Hzz + 2.0f * n.pxz * D::Hxz) * kInv2Cs4;
+            float A3 = 0.0f;
+            if constexpr (D::Hxxy != 0.0f) A3 += n.a3xxy * D::Hxxy;
+            if constexpr (D::Hxxz != 0.0f) A3 += n.a3xxz * D::Hxxz;
+            if constexpr (D::Hxyy != 0.0f) A3 += n.a3xyy * D::Hxyy;
+            if constexpr (D::Hxzz != 0.0f) A3 += n.a3xzz * D::Hxzz;
+            if constexpr (D::Hyyz != 0.0f) A3 += n.a3yyz * D::Hyyz;
+            if constexpr (D::Hyzz != 0.0f) A3 += n.a3yzz * D::Hyzz;
+            if constexpr (D::Hxyz != 0.0f) A3 += 2.0f * n.a3xyz * D::Hxyz;
+            A3 *= kInv2Cs6;
+            float o2A = 0.0f;  // Omega2 / (A/2), even
+            if (interface) o2A = absF * (D::w * (fc * fc) * invF2 - D::B);
+            const float Ge = wr * E + oms * D::w * A2 + (interface ? Ah * o2A : 0.0f);
+            const float Go = wr * O + oms * D::w * A3;
+            l_d += ds * Ge + dd * Go;
+            l_rhoeq += wr * (gs * E + gd * O);
+            // dfeq/du = w rho (c P - u Q): P = Pe +- Po, Q = 1/cs2 +- cu/cs4
+            const float Pe = kInvCs2 + (cu * cu) * (3.0f * kInv6Cs6) - usq * kInv2Cs4;
+            const float Po = cu * (2.0f * kInv2Cs4);
+            const float cP = wr * (gd * Pe + gs * Po);
+            if constexpr (D::cx != 0) l_uPx += D::fx * cP;
+            if constexpr (D::cy != 0) l_uPy += D::fy * cP;
+            if constexpr (D::cz != 0) l_uPz += D::fz * cP;
+            l_uQ += wr * (gs * kInvCs2 + gd * Po);
+            l_oms += D::w * (gs * A2 + gd * A3);
+            const float me = gs * D::w, mo = gd * D::w;
+            S2[0] += me * D::Hxx; S2[2] += me * D::Hyy; S2[4] += me * D::Hzz;
+            if constexpr (D::Hxy != 0.0f) S2[1] += me * D::Hxy;
+            if constexpr (D::Hyz != 0.0f) S2[3] += me * D::Hyz;
+            if constexpr (D::Hxz != 0.0f) S2[5] += me * D::Hxz;
+            if constexpr (D::Hxxy != 0.0f) S3[0] += mo * D::Hxxy;
+            if constexpr (D::Hxxz != 0.0f) S3[1] += mo * D::Hxxz;
+            if constexpr (D::Hxyy != 0.0f) S3[2] += mo * D::Hxyy;
+            if constexpr (D::Hxzz != 0.0f) S3[3] += mo * D::Hxzz;
+            if constexpr (D::Hyyz != 0.0f) S3[4] += mo * D::Hyyz;
+            if constexpr (D::Hyzz != 0.0f) S3[5] += mo * D::Hyzz;
+            if constexpr (D::Hxyz != 0.0f) S3[6] += mo * D::Hxyz;
             if (interface) {
-                const float cos2 = (i != 0 && has_dir) ? fc * fc * invF * invF : 0.0f;
-                om2_over_Ah = absF * (D::w * cos2 - D::B);
-                om2 = ph.Ah * om2_over_Ah;
-                if (i != 0 && has_dir) dlt = K * D::w * D::invc * fc * invF;
-            }
-            const float gi = fe + oms * fn + om2;
-            l_aR += lr * gi;
-            l_aB += lb * gi;
-            const float lg = aR * lr + aB * lb;
-            const float ld = lr - lb;
-            l_rhoeq += lg * fe;
-            // d feq / d u = w rho [c P - u Q]
-            const float P = kInvCs2 + cu * (2.0f * kInv2Cs4) + (cu * cu) * (3.0f * kInv6Cs6) - e.usq * kInv2Cs4;
-            const float Q = kInvCs2 + cu * (2.0f * kInv2Cs4);
-            const float wl = lg * D::w * rho;
-            if constexpr (D::cx != 0) l_uP[0] += wl * P * D::fx;
-            if constexpr (D::cy != 0) l_uP[1] += wl * P * D::fy;
-            if constexpr (D::cz != 0) l_uP[2] += wl * P * D::fz;
-            l_uQ += wl * Q;
-            l_oms += lg * fn;
-            const float mu = oms * lg * D::w;
-            S2[0] += mu * D::Hxx; S2[1] += mu * D::Hxy; S2[2] += mu * D::Hyy;
-            S2[3] += mu * D::Hyz; S2[4] += mu * D::Hzz; S2[5] += mu * D::Hxz;
-            if constexpr (D::Hxxy != 0.0f) S3[0] += mu * D::Hxxy;
-            if constexpr (D::Hxxz != 0.0f) S3[1] += mu * D::Hxxz;
-            if constexpr (D::Hxyy != 0.0f) S3[2] += mu * D::Hxyy;
-            if constexpr (D::Hxzz != 0.0f) S3[3] += mu * D::Hxzz;
-            if constexpr (D::Hyyz != 0.0f) S3[4] += mu * D::Hyyz;
-            if constexpr (D::Hyzz != 0.0f) S3[5] += mu * D::Hyzz;
-            if constexpr (D::Hxyz != 0.0f) S3[6] += mu * D::Hxyz;
-            if (interface) {
-                sBB += lg * D::B;
-                l_Ah += lg * om2_over_Ah;
-                if (i != 0 && has_dir) {
-                    const float a = lg * D::w * fc, d = ld * D::w * D::invc;
-                    if constexpr (D::cx != 0) { sA[0] += a * D::fx; sD[0] += d * D::fx; }
-                    if constexpr (D::cy != 0) { sA[1] += a * D::fy; sD[1] += d * D::fy; }
-                    if constexpr (D::cz != 0) { sA[2] += a * D::fz; sD[2] += d * D::fz; }
-                    sB += lg * D::w * fc * fc;
-                    sE += d * fc;
-                }
+                sBB += gs * D::B;
+                l_Ah += gs * o2A;
+                const float a = gs * D::w * fc, d = dd * D::w * D::invc;
+                if constexpr (D::cx != 0) { sAx += D::fx * a; sDx += D::fx * d; }
+                if constexpr (D::cy != 0) { sAy += D::fy * a; sDy += D::fy * d; }
+                if constexpr (D::cz != 0) { sAz += D::fz * a; sDz += D::fz * d; }
+                sB += a * fc;
+                sE += d * fc;
             }
         });
         // fneq: Pi enters directly (H2) and through the third-order terms a3
-        const float c2 = kInv2Cs4, c3 = kInv2Cs6;
+        const float c2 = oms * kInv2Cs4, c3 = oms * kInv2Cs6;
         float lPxx = S2[0] * c2, lPxy = 2.0f * S2[1] * c2, lPyy = S2[2] * c2;
         float lPyz = 2.0f * S2[3] * c2, lPzz = S2[4] * c2, lPxz = 2.0f * S2[5] * c2;
         const float la_xxy = S3[0] * c3, la_xxz = S3[1] * c3, la_xyy = S3[2] * c3, la_xzz = S3[3] * c3;
         const float la_yyz = S3[4] * c3, la_yzz = S3[5] * c3, la_xyz = 2.0f * S3[6] * c3;
-        float lux = 0.f, luy = 0.f, luz = 0.f;
         lPxx += la_xxy * uy + la_xxz * uz;
         lPyy += la_xyy * ux + la_yyz * uz;
         lPzz += la_xzz * ux + la_yzz * uy;
         lPxy += 2.0f * la_xxy * ux + 2.0f * la_xyy * uy + la_xyz * uz;
         lPxz += 2.0f * la_xxz * ux + 2.0f * la_xzz * uz + la_xyz * uy;
         lPyz += 2.0f * la_yyz * uy + 2.0f * la_yzz * uz + la_xyz * ux;
-        lux += 2.0f * la_xxy * n.pxy + 2.0f * la_xxz * n.pxz + la_xyy * n.pyy + la_xzz * n.pzz + la_xyz * n.pyz;
-        luy += la_xxy * n.pxx + 2.0f * la_xyy * n.pxy + 2.0f * la_yyz * n.pyz + la_yzz * n.pzz + la_xyz * n.pxz;
-        luz += la_xxz * n.pxx + 2.0f * la_xzz * n.pxz + la_yyz * n.pyy + 2.0f * la_yzz * n.pyz + la_xyz * n.pxy;
+        float lux = 2.0f * la_xxy * n.pxy + 2.0f * la_xxz * n.pxz + la_xyy * n.pyy + la_xzz * n.pzz + la_xyz * n.pyz;
+        float luy = la_xxy * n.pxx + 2.0f * la_xyy * n.pxy + 2.0f * la_yyz * n.pyz + la_yzz * n.pzz + la_xyz * n.pxz;
+        float luz = la_xxz * n.pxx + 2.0f * la_xzz * n.pxz + la_yyz * n.pyy + 2.0f * la_yzz * n.pyz + la_xyz * n.pxy;
         // feq
-        lux += l_uP[0] - ux * l_uQ;
-        luy += l_uP[1] - uy * l_uQ;
-        luz += l_uP[2] - uz * l_uQ;
+        lux += l_uPx - ux * l_uQ;
+        luy += l_uPy - uy * l_uQ;
+        luz += l_uPz - uz * l_uQ;
         // colour gradient: perturbation and recolouring
         float lFx = 0.f, lFy = 0.f, lFz = 0.f, lK = 0.f;
         if (interface) {
-            const float ah = ph.Ah;
             if (has_dir) {
-                const float i3 = invF * invF * invF;
-                lFx = ah * (2.0f * invF * sA[0] - Fx * i3 * sB - Fx * invF * sBB) + K * (sD[0] * invF - Fx * i3 * sE);
-                lFy = ah * (2.0f * invF * sA[1] - Fy * i3 * sB - Fy * invF * sBB) + K * (sD[1] * invF - Fy * i3 * sE);
-                lFz = ah * (2.0f * invF * sA[2] - Fz * i3 * sB - Fz * invF * sBB) + K * (sD[2] * invF - Fz * i3 * sE);
+                const float i3 = invF2 * invF;
+                lFx = Ah * (2.0f * invF * sAx - Fx * i3 * sB - Fx * invF * sBB) + K * (sDx * invF - Fx * i3 * sE);
+                lFy = Ah * (2.0f * invF * sAy - Fy * i3 * sB - Fy * invF * sBB) + K * (sDy * invF - Fy * i3 * sE);
+                lFz = Ah * (2.0f * invF * sAz - Fz * i3 * sB - Fz * invF * sBB) + K * (sDz * invF - Fz * i3 * sE);
                 lK = sE * invF;
             } else if (absF > 0.0f) {
-                const float q = -ah * sBB / absF;
+                const float q = -Ah * sBB / absF;
                 lFx = q * Fx;
                 lFy = q * Fy;
                 lFz = q * Fz;
@@ -1256,10 +1314,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, 
         }
         const float inv2 = invr * invr;
         const float l_rho = l_rhoeq * invr;  // feq is proportional to rho
-        const float lrr = l_rho + (l_aR - l_aB) * rb * inv2 + lK * ph.beta * rb * rb * inv2;
-        const float lrb = l_rho - (l_aR - l_aB) * rr * inv2 + lK * ph.beta * rr * rr * inv2;
-        lmom[kMomRR * N + id] = lrr;
-        lmom[kMomRB * N + id] = lrb;
+        lmom[kMomRR * N + id] = l_rho + l_d * rb * inv2 + lK * ph.beta * rb * rb * inv2;
+        lmom[kMomRB * N + id] = l_rho - l_d * rr * inv2 + lK * ph.beta * rr * rr * inv2;
         lmom[kMomUX * N + id] = lux;
         lmom[kMomUY * N + id] = luy;
         lmom[kMomUZ * N + id] = luz;
@@ -1286,8 +1342,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_collide(const DeviceState s, 
 // Per node: the psi-adjoint gathered from the neighbours' F-adjoints, then back
 // through the moments to the 54 pulled populations, stored at their pull
 // sources (transposed streaming) in lam_out.
-__global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *lmom, const float *lf,
-                                                          float *lam_out) {
+__global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *__restrict__ M,
+                                                          const float *lmom, const float *lf, float *lam_out) {
     const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
@@ -1295,7 +1351,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
     const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
     const size_t N = g.N;
-    const float *mom = s.mom;
+    const float *mom = M;
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const float rho = rr + rb;
@@ -1350,7 +1406,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
 
 // dJ/du0 for an initial state f0_c,i = feq_i(rho_c, u0): pulls lambda_0 like
 // the forward step pulls populations.
-__global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, const float *lam0, float *du0) {
+__global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, const float *__restrict__ M,
+                                                          const float *lam0, float *du0) {
     const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
@@ -1362,7 +1419,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, 
         du0[id] = du0[N + id] = du0[2 * N + id] = 0.0f;
         return;
     }
-    const float *mom = s.mom;
+    const float *mom = M;
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const EqTerms e = make_eq(ux, uy, uz);
@@ -1543,22 +1600,23 @@ cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_terminal(const DeviceState &s, const float *target, float *lam, double *J, cudaStream_t st) {
-    k_adj_terminal<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, target, lam, J);
+cudaError_t launch_adj_terminal(const DeviceState &s, const float *M, const float *target, float *lam, double *J,
+                                cudaStream_t st) {
+    k_adj_terminal<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, target, lam, J);
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_step(const DeviceState &s, int64_t step, const float *lam_in, float *lmom, float *lf,
+cudaError_t launch_adj_step(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
                             float *lam_out, double *acc, cudaStream_t st) {
-    k_adj_collide<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, step, lam_in, lmom, lf, acc);
+    k_adj_collide<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lam_in, lmom, lf, acc);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_adj_moments<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, lmom, lf, lam_out);
+    k_adj_moments<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lmom, lf, lam_out);
     return cudaGetLastError();
 }
 
-cudaError_t launch_adj_initial(const DeviceState &s, const float *lam0, float *du0, cudaStream_t st) {
-    k_adj_initial<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, lam0, du0);
+cudaError_t launch_adj_initial(const DeviceState &s, const float *M, const float *lam0, float *du0, cudaStream_t st) {
+    k_adj_initial<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lam0, du0);
     return cudaGetLastError();
 }
 

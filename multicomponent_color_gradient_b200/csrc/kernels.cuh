@@ -34,6 +34,8 @@ namespace mcg {
 enum : int { kBoundaryJet = 0, kBoundaryClosed = 1, kBoundaryPeriodic = 2 };
 enum : int { kStoreF32 = 0, kStoreF16 = 1 };
 enum : int { kMomRR = 0, kMomRB, kMomUX, kMomUY, kMomUZ, kMomPXX, kMomPXY, kMomPYY, kMomPYZ, kMomPZZ, kMomPXZ, kMomCount };
+// A moment record of one state: the kMomCount moment planes, then psi.
+enum : int { kTapePsi = kMomCount, kTapePlanes = kMomCount + 1 };
 
 struct Geometry {
     int NX, NY, NZ;
@@ -93,6 +95,7 @@ struct DeviceState {
     double *partials; // reduction scratch
     uint32_t partials_cap;
     int *flag;        // device flag (non-finite detection)
+    float *tape;      // null, or [kTapePlanes][N]: the fused step records the moments and psi it pulls there
 };
 
 // ---- the fused step (moments + colour gradient + collision in one pass) ----
@@ -134,14 +137,15 @@ cudaError_t launch_conservation(const DeviceState &s, int cur, double *partials,
 cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaStream_t st);
 
 // ---- discrete adjoint of the step (periodic box, float32 populations) ----
-// lambda buffers share the population layout.  Terminal condition for
-// J = sum (psi_T - target)^2 (needs the moment planes of S_T), one adjoint step
-// (needs the moment planes and psi of S_t; lmom [11][N], lf [3][N] scratch;
-// acc[0] += dJ/domega, acc[1] += dJ/d(A/2)), and dJ/du0 of a state
-// f0 = feq(rho_c, u0) (needs the moment planes of S_0; du0 [3][N]).
-cudaError_t launch_adj_terminal(const DeviceState &s, const float *target, float *lam, double *J, cudaStream_t st);
-cudaError_t launch_adj_step(const DeviceState &s, int64_t step, const float *lam_in, float *lmom, float *lf,
+// lambda buffers share the population layout; M is the moment record
+// [kTapePlanes][N] of the state the pass belongs to (interior nodes).
+// Terminal condition for J = sum (psi_T - target)^2, one adjoint step
+// (lmom [11][N], lf [3][N] scratch; acc[0] += dJ/domega, acc[1] += dJ/d(A/2)),
+// and dJ/du0 of a state f0 = feq(rho_c, u0) (du0 [3][N]).
+cudaError_t launch_adj_terminal(const DeviceState &s, const float *M, const float *target, float *lam, double *J,
+                                cudaStream_t st);
+cudaError_t launch_adj_step(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
                             float *lam_out, double *acc, cudaStream_t st);
-cudaError_t launch_adj_initial(const DeviceState &s, const float *lam0, float *du0, cudaStream_t st);
+cudaError_t launch_adj_initial(const DeviceState &s, const float *M, const float *lam0, float *du0, cudaStream_t st);
 
 }  // namespace mcg
