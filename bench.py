@@ -175,6 +175,31 @@ def cpu_baseline(case_name: str, steps: int):
             "sample": f"{steps} steps of {case_name} (float64 OpenMP oracle, radial statistics on), {dt:.1f} s"}
 
 
+def adjoint_cost(steps: int):
+    """Discrete-adjoint cost on the 96^3 periodic bubble (R=20, tau 0.7, sigma
+    0.01): device time of one forward + reverse sweep over `steps` steps (a
+    moment record per state) against `steps` plain forward steps."""
+    import numpy as np
+
+    from multicomponent_color_gradient_b200.adjoint import BubbleProblem
+
+    P = BubbleProblem("adjoint_bubble_96", nsteps=steps, max_mode=1, seed=1, relax_steps=0)
+    try:
+        a = np.random.default_rng(2).normal(scale=2e-3, size=P.modes.count)
+        P.evaluate(a)
+        r = P.evaluate(a)
+        S = P.solver(P.case["sigma"], P.case["taub"])
+        u = P.initial_velocity(a)
+        S.init_equilibrium(P.rhor, P.rhob, u[0], u[1], u[2])
+        S.step(3)
+        fwd = S.step_timed(steps)
+        return {"value": round(r["ms"] / fwd, 3), "unit": "adjoint sweep / forward run", "workload": "adjoint_bubble_96",
+                "steps": steps, "sweep_ms": round(r["ms"], 3), "forward_ms": round(fwd, 3),
+                "forward_steps_in_sweep": r["forward_steps"]}
+    finally:
+        P.close()
+
+
 def run_reference(args, world, rank):
     if world > 1 and rank != 0:
         return
@@ -223,6 +248,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost measurement")
+    ap.add_argument("--adjoint-steps", type=int, default=100)
     ap.add_argument("--shape", default=None,
                     help="NXxNYxNZ override of the case grid (smaller profiling captures); not a bench line")
     args = ap.parse_args()
@@ -319,6 +346,13 @@ def main():
                "step_frac_216B": round(216 * cells / (ms16 / args.steps * 1e-3) / 1e9 / hbm_peak, 4)}
         S16.close()
 
+    adjoint = None
+    if not args.no_adjoint:
+        try:
+            adjoint = adjoint_cost(args.adjoint_steps)
+        except Exception as exc:
+            adjoint = {"value": None, "error": str(exc)[:200]}
+
     if rank != 0:
         return
     cpu = None
@@ -337,7 +371,7 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (step_bytes / 2 * cells / 1e6)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-        "f16_store": f16,
+        "f16_store": f16, "adjoint": adjoint,
     }
     print(json.dumps(line))
 
