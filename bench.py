@@ -158,8 +158,9 @@ def max_over_ranks(world, v: float) -> float:
     return float(t.item())
 
 
-def cpu_baseline(case_name: str, steps: int):
-    """Float64 OpenMP oracle on a sample of the same workload (rank 0 only)."""
+def cpu_baseline(case_name: str, seconds: float):
+    """Float64 OpenMP oracle on a sample of the same workload (rank 0 only):
+    whole steps until `seconds` of host time have passed."""
     from multicomponent_color_gradient_b200 import get_case
     from oracle.oracle import Oracle, num_threads
 
@@ -167,9 +168,14 @@ def cpu_baseline(case_name: str, steps: int):
     O = Oracle(case, 64)
     O.init_jet()
     O.step(1)  # warm-up (first touch of the arrays)
+    steps = 0
     t0 = time.perf_counter()
-    O.step(steps)
-    dt = time.perf_counter() - t0
+    while True:
+        O.step(1)
+        steps += 1
+        dt = time.perf_counter() - t0
+        if dt >= seconds:
+            break
     cells = case["NX"] * case["NY"] * case["NZ"]
     return {"value": round(cells * steps / dt / 1e6, 3), "unit": "MLUPS", "cores": num_threads(), "kind": "port",
             "sample": f"{steps} steps of {case_name} (float64 OpenMP oracle, radial statistics on), {dt:.1f} s"}
@@ -245,7 +251,7 @@ def main():
     ap.add_argument("--case", default=DEFAULT_CASE)
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
     ap.add_argument("--no-f16", action="store_true", help="skip the float16-storage companion measurement")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="host time of the cpu_baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost measurement")
@@ -358,7 +364,7 @@ def main():
     cpu = None
     if not args.no_cpu:
         try:
-            cpu = cpu_baseline(args.case, args.cpu_steps)
+            cpu = cpu_baseline(args.case, args.cpu_seconds)
         except Exception as exc:
             cpu = {"value": None, "error": str(exc)[:200]}
     line = {
