@@ -231,6 +231,28 @@ __constant__ int c_cz[kQ] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1,
 
 // ------------------------------------------------------------------ per-node pieces
 
+// Colour densities only of interior node (x,y,z): the sums of pull_moments
+// below in the same order, so psi formed from them is bit-identical.  Nodes
+// whose psi is all that is needed (halo rows and planes of a tile) take this.
+template <class C, bool kPeriodic>
+__device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec, int x, int y, int z, float &rr,
+                                               float &rb) {
+    const PullMap<C> pm(g, x, y, z, kPeriodic);
+    float sumr = 0.f, sumb = 0.f;
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        size_t grow;
+        int xs;
+        pm.template src<i>(x, grow, xs);
+        float fr, fb;
+        codec.template load<i>(grow, xs, fr, fb);
+        sumr += fr;
+        sumb += fb;
+    });
+    rr = sumr;
+    rb = sumb;
+}
+
 // Pull the 54 populations of interior node (x,y,z) and form its moments
 // (lbm.cuh:106-164, same summation order).
 template <class C, bool kPeriodic>
@@ -472,10 +494,14 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
                     pull = xin && y >= 1 && y <= g.NY - 2 && zp >= 1 && zp <= g.NZ - 2;
                 }
                 float ps;
-                if (pull) {
+                if (pull && own_row) {  // uniform per warp: a warp covers part of one row
                     m = pull_moments<C, kPeriodic>(g, codec, xn, yn, zn);
                     have = true;
                     ps = psi_of(m.rr, m.rb);
+                } else if (pull) {
+                    float rr, rb;
+                    pull_densities<C, kPeriodic>(g, codec, xn, yn, zn, rr, rb);
+                    ps = psi_of(rr, rb);
                 } else {
                     ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
                 }
