@@ -44,10 +44,17 @@ constexpr unsigned kFull = 0xffffffffu;
 // ------------------------------------------------------------------ storage codecs
 
 struct CodecF32 {
+    using Elem = float;
     static constexpr int kGroupSlots = 6;
     const float *__restrict__ rd;
     float *__restrict__ wr;
     int NX;
+    // store through `wrow` = the node's row in the written buffer, offset by x
+    template <int I>
+    __device__ __forceinline__ void store_row(float *wrow, float r, float b) const {
+        wrow[slot_f32(I, 0) * NX] = r;
+        wrow[slot_f32(I, 1) * NX] = b;
+    }
     // pull: `grow` = offset of the source row's group segment
     template <int I>
     __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
@@ -95,11 +102,16 @@ __device__ __forceinline__ void f16_decode(__half2 h, float w, float rho0, float
 }
 
 struct CodecF16 {
+    using Elem = __half2;
     static constexpr int kGroupSlots = 3;
     const __half2 *__restrict__ rd;
     __half2 *__restrict__ wr;
     int NX;
     float rho0;
+    template <int I>
+    __device__ __forceinline__ void store_row(__half2 *wrow, float r, float b) const {
+        wrow[slot_f16(I) * NX] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
+    }
     template <int I>
     __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
         const __half2 h = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
@@ -302,35 +314,29 @@ __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &
 }
 
 // Relax one node and store its 54 post-collision values (lbm.cuh:184-293).
-// Opposite directions are evaluated together: equilibrium and regularised
-// non-equilibrium split into even and odd parts, the perturbation Omega2 is
-// even (cos^2) and the recolouring Delta odd (cos phi).  psi_at(cx,cy,cz)
-// returns the neighbour's psi, read unwrapped like forces.cuh:31 (ghost psi
-// is what the reference sees there).
+// The bulk part feq + (1-omega) fneq of all 27 directions comes from
+// collision_poly (lattice.cuh).  At interface nodes the perturbation Omega2
+// (even in c: one evaluation per opposite pair) and the recolouring Delta
+// (odd) are added per direction.  psi_at(cx,cy,cz) returns the neighbour's
+// psi, read unwrapped like forces.cuh:31 (ghost psi is what the reference
+// sees there).
 template <class C, class PsiAt>
 __device__ __forceinline__ void collide_node(const Geometry &g, const Physics &ph, const C &codec, size_t row, int x,
                                              int y, int z, const NodeMoments &m, PsiAt &&psi_at) {
     const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
-    const EqTerms e = make_eq(m.ux, m.uy, m.uz);
     const float rr = m.rr, rb = m.rb;
     const float rT = rr + rb;
     const float invrT = 1.0f / rT;
     const float aR = rr * invrT, aB = rb * invrT;
     const float oms = 1.0f - omega_at(ph, y);
     const float Iind = 4.0f * rr * rb * invrT * invrT;
+    float P[kQ];
+    collision_poly(rT, m.ux, m.uy, m.uz, n, oms, P);
+    typename C::Elem *const wrow = codec.wr + row + x;
     if (Iind <= 1e-4f) {  // bulk (lbm.cuh:216-247)
-        {
-            const float g0 = feq<0>(rT, e) + oms * fneq<0>(n);
-            codec.template store<0>(row, x, aR * g0, aB * g0);
-        }
-        static_for<(kQ - 1) / 2>([&](auto P) {
-            constexpr int i = 2 * decltype(P)::value + 1;
-            float ei, eo, ni, no;
-            feq_pair<i>(rT, e, ei, eo);
-            fneq_pair<i>(n, ni, no);
-            const float gi = ei + oms * ni, go = eo + oms * no;
-            codec.template store<i>(row, x, aR * gi, aB * gi);
-            codec.template store<i + 1>(row, x, aR * go, aB * go);
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            codec.template store_row<i>(wrow, (aR * Dir<i>::w) * P[i], (aB * Dir<i>::w) * P[i]);
         });
         return;
     }
@@ -358,19 +364,16 @@ __device__ __forceinline__ void collide_node(const Geometry &g, const Physics &p
     t.Ah_absF = ph.Ah * t.absF;
     t.coeff_rho = ph.beta * ((rr * rb) / (rT * rT)) * rT;
     {
-        const float g0 = feq<0>(rT, e) + oms * fneq<0>(n) + omega2<0>(t);
-        codec.template store<0>(row, x, aR * g0, aB * g0);
+        const float g0 = Dir<0>::w * P[0] + omega2<0>(t);
+        codec.template store_row<0>(wrow, aR * g0, aB * g0);
     }
-    static_for<(kQ - 1) / 2>([&](auto P) {
-        constexpr int i = 2 * decltype(P)::value + 1;
-        float ei, eo, ni, no;
-        feq_pair<i>(rT, e, ei, eo);
-        fneq_pair<i>(n, ni, no);
+    static_for<(kQ - 1) / 2>([&](auto Q) {
+        constexpr int i = 2 * decltype(Q)::value + 1;
         const float o2 = omega2<i>(t);  // even: the same for i and its opposite
-        const float gi = ei + oms * ni + o2, go = eo + oms * no + o2;
+        const float gi = Dir<i>::w * P[i] + o2, go = Dir<i + 1>::w * P[i + 1] + o2;
         const float d = recolour<i>(t);  // odd: -d for the opposite
-        codec.template store<i>(row, x, aR * gi + d, aB * gi - d);
-        codec.template store<i + 1>(row, x, aR * go - d, aB * go + d);
+        codec.template store_row<i>(wrow, aR * gi + d, aB * gi - d);
+        codec.template store_row<i + 1>(wrow, aR * go - d, aB * go + d);
     });
 }
 

@@ -47,6 +47,13 @@ __host__ __device__ constexpr float dir_w(int i) {
          : dir_norm2(i) == 2 ? float(1.0 / 54.0)
                              : float(1.0 / 216.0);
 }
+// Direction index of velocity (cx, cy, cz) (inverse of dir_cx/cy/cz).
+__host__ __device__ constexpr int dir_of(int cx, int cy, int cz) {
+    int r = -1;
+    for (int i = 0; i < kQ; ++i)
+        if (dir_cx(i) == cx && dir_cy(i) == cy && dir_cz(i) == cz) r = i;
+    return r;
+}
 __host__ __device__ constexpr float dir_B(int i) { return i == 0 ? float(-10.0 / 27.0) : dir_w(i); }
 __host__ __device__ constexpr float dir_invc(int i) {
     return dir_norm2(i) == 0 ? 0.0f
@@ -194,6 +201,73 @@ __device__ __forceinline__ void fneq_pair(const NeqTerms &n, float &fi, float &f
     A3 *= kInv2Cs6;
     fi = D::w * (A2 + A3);
     fo = D::w * (A2 - A3);
+}
+
+// Bulk post-collision value over the weight, P[i] = (feq_i + oms fneq_i) / w_i
+// (lbm.cuh:16-78), for all 27 directions at once.  As a function of c_i it is
+// the polynomial
+//   rho [1 + q u.c + (q^2/2)(u.c)^2 - (q/2)|u|^2 + (q^3/6)(u.c)^3 - (q^2/2)|u|^2 u.c]
+//   + oms [(q^2/2) Pi:(cc - I/q) + (q^3/2) sum_k a3_k H3_k(c)],      q = 1/cs^2,
+// which on the lattice (c_a^3 = c_a) has 17 coefficients of per-axis degree
+// <= 2.  D3Q27 is the tensor product of three D1Q3 stencils, so the 27 values
+// follow from the coefficients by three passes of 1-D evaluation at
+// c = -1, 0, 1 (sum factorisation): about 70 adds instead of a Hermite
+// evaluation per direction.
+__device__ __forceinline__ void collision_poly(float rho, float ux, float uy, float uz, const NeqTerms &n, float oms,
+                                               float (&P)[kQ]) {
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    const float usq = ux2 + uy2 + uz2;
+    const float lin = kInvCs2 - kInv2Cs4 * usq;
+    // coefficients of 1, c_a, c_a^2, c_a c_b, c_a^2 c_b, c_x c_y c_z
+    const float a0 = rho - kInv2Cs2 * (rho * usq + oms * (n.pxx + n.pyy + n.pzz));
+    const float Ax = rho * ux * (lin + kInv6Cs6 * ux2) - oms * kInv2Cs4 * (n.a3xyy + n.a3xzz);
+    const float Ay = rho * uy * (lin + kInv6Cs6 * uy2) - oms * kInv2Cs4 * (n.a3xxy + n.a3yzz);
+    const float Az = rho * uz * (lin + kInv6Cs6 * uz2) - oms * kInv2Cs4 * (n.a3xxz + n.a3yyz);
+    const float rx2 = rho * ux2, ry2 = rho * uy2, rz2 = rho * uz2;
+    const float Axx = kInv2Cs4 * (rx2 + oms * n.pxx);
+    const float Ayy = kInv2Cs4 * (ry2 + oms * n.pyy);
+    const float Azz = kInv2Cs4 * (rz2 + oms * n.pzz);
+    const float Axy = (2.0f * kInv2Cs4) * (rho * ux * uy + oms * n.pxy);
+    const float Axz = (2.0f * kInv2Cs4) * (rho * ux * uz + oms * n.pxz);
+    const float Ayz = (2.0f * kInv2Cs4) * (rho * uy * uz + oms * n.pyz);
+    const float Axxy = kInv2Cs6 * (rx2 * uy + oms * n.a3xxy);
+    const float Axxz = kInv2Cs6 * (rx2 * uz + oms * n.a3xxz);
+    const float Ayyx = kInv2Cs6 * (ry2 * ux + oms * n.a3xyy);
+    const float Azzx = kInv2Cs6 * (rz2 * ux + oms * n.a3xzz);
+    const float Ayyz = kInv2Cs6 * (ry2 * uz + oms * n.a3yyz);
+    const float Azzy = kInv2Cs6 * (rz2 * uy + oms * n.a3yzz);
+    const float Axyz = (2.0f * kInv2Cs6) * (rho * ux * uy * uz + oms * n.a3xyz);
+    // P = B0(cx,cy) + cz B1(cx,cy) + cz^2 B2(cx,cy); B* = C*(cx) + cy C*'(cx) + cy^2 C*''(cx)
+    float C0[3], C1[3], C2[3], D0[3], D1[3], E0[3];
+    {
+        const float s = a0 + Axx;
+        C0[0] = s - Ax; C0[1] = a0; C0[2] = s + Ax;
+    }
+    {
+        const float s = Ay + Axxy;
+        C1[0] = s - Axy; C1[1] = Ay; C1[2] = s + Axy;
+    }
+    C2[0] = Ayy - Ayyx; C2[1] = Ayy; C2[2] = Ayy + Ayyx;
+    {
+        const float s = Az + Axxz;
+        D0[0] = s - Axz; D0[1] = Az; D0[2] = s + Axz;
+    }
+    D1[0] = Ayz - Axyz; D1[1] = Ayz; D1[2] = Ayz + Axyz;
+    E0[0] = Azz - Azzx; E0[1] = Azz; E0[2] = Azz + Azzx;
+    static_for<3>([&](auto JX) {
+        constexpr int jx = decltype(JX)::value;
+        const float b0s = C0[jx] + C2[jx], b1s = D0[jx] + Ayyz;
+        const float b0[3] = {b0s - C1[jx], C0[jx], b0s + C1[jx]};
+        const float b1[3] = {b1s - D1[jx], D0[jx], b1s + D1[jx]};
+        const float b2[3] = {E0[jx] - Azzy, E0[jx], E0[jx] + Azzy};
+        static_for<3>([&](auto JY) {
+            constexpr int jy = decltype(JY)::value;
+            const float t = b0[jy] + b2[jy];
+            P[dir_of(jx - 1, jy - 1, 0)] = b0[jy];
+            P[dir_of(jx - 1, jy - 1, -1)] = t - b1[jy];
+            P[dir_of(jx - 1, jy - 1, 1)] = t + b1[jy];
+        });
+    });
 }
 
 // Interface terms shared by all directions of one node.
