@@ -436,6 +436,31 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
 // ------------------------------------------------------------------ the fused step
 
 constexpr int kFusedThreads = 256;
+
+// L2 prefetch of the populations that node row (y, z) pulls: one bulk
+// prefetch (cp.async.bulk.prefetch.L2, no shared memory, no completion to wait
+// for) per (cy, cz) group segment of its nine source rows.  `k` in [0, 9)
+// picks the group.  Rows whose pull does not happen (a y ghost row of the
+// closed or jet box) are skipped; sources follow the same wrap and ghost rules
+// as PullMap, so every address lies inside the buffer.
+template <class C, bool kPeriodic>
+__device__ __forceinline__ void prefetch_pull_group(const Geometry &g, const C &codec, int y, int z, int k) {
+    int yn = y, zn = z;
+    if constexpr (kPeriodic) {
+        yn = wrap_interior(y, g.NY);
+        zn = wrap_interior(z, g.NZ);
+    } else {
+        if (y < 1 || y > g.NY - 2 || z < 1 || z > g.NZ - 2) return;
+    }
+    const int cy = k / 3 - 1, cz = k % 3 - 1;
+    int ys = yn - cy, zs = zn - cz;
+    const bool ghost = !kPeriodic && (ys == 0 || ys == g.NY - 1);
+    if (kPeriodic) ys = wrap_interior(ys, g.NY);
+    if (!ghost) zs = wrap_interior(zs, g.NZ);
+    const typename C::Elem *p = codec.rd + pop_row(g, ys, zs) + size_t(k * C::kGroupSlots) * size_t(g.NX);
+    const uint32_t bytes = uint32_t(C::kGroupSlots * g.NX * sizeof(typename C::Elem));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 #ifndef MCG_FUSED_MIN_BLOCKS
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
@@ -474,10 +499,22 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     const float *nbr_lo = lower_nbr ? cluster.map_shared_rank(ring, crank - 1) : nullptr;
     const float *nbr_hi = upper_nbr ? cluster.map_shared_rank(ring, crank + 1) : nullptr;
 
-    for (int zp = z0 - 1; zp <= z0 + lz; ++zp) {
+    // Odd chunks march down: the plane two neighbouring chunks both pull (one
+    // as its halo, one as its own) is then pulled by both at the same end of
+    // their marches, close in time, and the second pull finds it in L2.
+    const bool down = T.alternate && (blockIdx.y & 1);
+    for (int k = 0; k <= lz + 1; ++k) {
+        const int zp = down ? z0 + lz - k : z0 - 1 + k;
         float *ringp = ring + (zp % 3) * pstride;
         float *msmp = msm + (zp & 1) * mplane;
         const bool own_plane = zp >= z0 && zp < z0 + lz;
+        if (T.prefetch > 0) {
+            // the rows of the plane `prefetch` steps ahead that this tile will pull
+            const int zf = down ? zp - T.prefetch : zp + T.prefetch;
+            const int nseg = 9 * (ty + 2);
+            if (zf >= z0 - 1 && zf <= z0 + lz && int(threadIdx.x) < nseg)
+                prefetch_pull_group<C, kPeriodic>(g, codec, y0 - 1 + int(threadIdx.x) / 9, zf, int(threadIdx.x) % 9);
+        }
         // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
         for (int r = lr; r < ty + 2; r += rpt) {
             if ((r == 0 && lower_nbr) || (r == ty + 1 && upper_nbr)) continue;  // from a neighbour below
@@ -558,8 +595,8 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
             }
         }
         __syncthreads();
-        // ---- relax plane zp-1 with psi of planes zp-2 .. zp
-        const int zc = zp - 1;
+        // ---- relax the plane behind the march front, whose neighbours are all pulled
+        const int zc = down ? zp + 1 : zp - 1;
         if (zc >= z0 && zc < z0 + lz) {
             const float *pm = ring + ((zc + 2) % 3) * pstride;  // plane zc-1
             const float *p0 = ring + (zc % 3) * pstride;        // plane zc
@@ -1516,6 +1553,13 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     t.lz = lz;
     t.nz_chunks = (g.NZ - 2 + lz - 1) / lz;
     t.smem_bytes = (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
+    // bulk prefetch needs 16-byte aligned segments of a multiple of 16 bytes:
+    // NX even (float32 rows of 6 NX floats) or a multiple of 4 (float16, 3 NX words)
+    t.prefetch = 0;
+    if (const char *v = std::getenv("MCG_FUSED_PREFETCH")) t.prefetch = std::max(0, std::atoi(v));  // tuning sweeps
+    if (g.NX % (g.storage == kStoreF16 ? 4 : 2) != 0) t.prefetch = 0;
+    t.alternate = 1;
+    if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
     return t;
 }
 

@@ -72,7 +72,8 @@ struct Physics {
 };
 
 // Tiling of the fused step: a CTA owns rows [y0, y0+ty) of every plane of a
-// z-chunk [z0, z0+lz) and marches z; tpr threads per row (a multiple of 32,
+// z-chunk [z0, z0+lz) and marches z (up, or down for odd chunks when
+// `alternate`); tpr threads per row (a multiple of 32,
 // >= NX), blockDim.x / tpr rows in parallel.  `cluster` consecutive y-tiles
 // form a thread-block cluster that exchanges edge psi rows through
 // distributed shared memory, so only the cluster's outer halo rows are pulled.
@@ -81,6 +82,8 @@ struct FusedTiling {
     int ny_tiles, nz_chunks;
     int cluster;
     int smem_bytes;
+    int prefetch;  // planes ahead whose source rows are prefetched into L2 (0: off)
+    int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
 };
 
 struct DeviceState {
