@@ -465,6 +465,106 @@ __device__ __forceinline__ void prefetch_pull_group(const Geometry &g, const C &
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
 
+// One node of a tile row in plane zp, pulled: psi into `ring_row` (all
+// columns, halo rows included), and for own rows the moments into `msm_row`,
+// the fluid-plane moments for the boundary launch, the adjoint's moment
+// record, and the radial statistics.  Warp-collective when kStats: all 32
+// lanes of a warp (one row) call it together.
+template <class C, bool kStats, bool kPeriodic>
+__device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, const float *__restrict__ psi_g, int x,
+                                          int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr) {
+    const Geometry &g = s.g;
+    const bool xin = x >= 1 && x <= g.NX - 2;
+    NodeMoments m{};
+    bool have = false;
+    if (x < g.NX) {
+        int xn = x, yn = y, zn = zp;
+        bool pull;
+        if constexpr (kPeriodic) {
+            xn = wrap_interior(x, g.NX);
+            yn = wrap_interior(y, g.NY);
+            zn = wrap_interior(zp, g.NZ);
+            pull = true;
+        } else {
+            pull = xin && y >= 1 && y <= g.NY - 2 && zp >= 1 && zp <= g.NZ - 2;
+        }
+        float ps;
+        if (pull && own_row) {  // uniform per warp: a warp covers part of one row
+            m = pull_moments<C, kPeriodic>(g, codec, xn, yn, zn);
+            have = true;
+            ps = psi_of(m.rr, m.rb);
+        } else if (pull) {
+            float rr, rb;
+            pull_densities<C, kPeriodic>(g, codec, xn, yn, zn, rr, rb);
+            ps = psi_of(rr, rb);
+        } else {
+            ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
+        }
+        ring_row[x] = ps;
+        if (own_row && xin) {
+            float *q = msm_row + x;
+            q[kMomRR * tpr] = m.rr;
+            q[kMomRB * tpr] = m.rb;
+            q[kMomUX * tpr] = m.ux;
+            q[kMomUY * tpr] = m.uy;
+            q[kMomUZ * tpr] = m.uz;
+            q[kMomPXX * tpr] = m.pxx;
+            q[kMomPXY * tpr] = m.pxy;
+            q[kMomPYY * tpr] = m.pyy;
+            q[kMomPYZ * tpr] = m.pyz;
+            q[kMomPZZ * tpr] = m.pzz;
+            q[kMomPXZ * tpr] = m.pxz;
+            if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
+                // fluid-plane moments for the boundary launch
+                float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
+                const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
+#pragma unroll
+                for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
+            }
+            if (std::is_same<C, CodecF32>::value && kPeriodic && s.tape) {
+                // moment record of the pulled state (the adjoint sweep reads it)
+                float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
+                const size_t N = g.N;
+                const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, ps};
+#pragma unroll
+                for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
+            }
+        }
+    }
+    if constexpr (kStats) {
+        if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
+    }
+}
+
+// Relax interior node (x, y, zc) of a tile: moments from the stage row
+// `msm_row`, psi of planes zc-1, zc, zc+1 from the ring planes pm, p0, pp at
+// ring row r.
+template <class C>
+__device__ __forceinline__ void tile_collide(const DeviceState &s, const C &codec, int x, int y, int zc, int r,
+                                             const float *msm_row, const float *pm, const float *p0, const float *pp,
+                                             int tpr) {
+    const Geometry &g = s.g;
+    const float *q = msm_row + x;
+    NodeMoments m;
+    m.rr = q[kMomRR * tpr];
+    m.rb = q[kMomRB * tpr];
+    m.ux = q[kMomUX * tpr];
+    m.uy = q[kMomUY * tpr];
+    m.uz = q[kMomUZ * tpr];
+    m.pxx = q[kMomPXX * tpr];
+    m.pxy = q[kMomPXY * tpr];
+    m.pyy = q[kMomPYY * tpr];
+    m.pyz = q[kMomPYZ * tpr];
+    m.pzz = q[kMomPZZ * tpr];
+    m.pxz = q[kMomPXZ * tpr];
+    const int base = r * tpr + x;
+    auto psi_at = [&](int cx, int cy, int cz) {
+        const float *pl = cz < 0 ? pm : (cz > 0 ? pp : p0);
+        return pl[base + cy * tpr + cx];
+    };
+    collide_node(g, s.ph, codec, pop_row(g, y, zc), x, y, zc, m, psi_at);
+}
+
 template <class C, bool kStats, bool kPeriodic>
 __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(const DeviceState s, const FusedTiling T, int cur,
                                                             int64_t step) {
@@ -518,69 +618,8 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
         for (int r = lr; r < ty + 2; r += rpt) {
             if ((r == 0 && lower_nbr) || (r == ty + 1 && upper_nbr)) continue;  // from a neighbour below
-            const int y = y0 - 1 + r;
-            const bool own_row = own_plane && r >= 1 && r <= ty;
-            NodeMoments m{};
-            bool have = false;
-            if (x < g.NX) {
-                int xn = x, yn = y, zn = zp;
-                bool pull;
-                if constexpr (kPeriodic) {
-                    xn = wrap_interior(x, g.NX);
-                    yn = wrap_interior(y, g.NY);
-                    zn = wrap_interior(zp, g.NZ);
-                    pull = true;
-                } else {
-                    pull = xin && y >= 1 && y <= g.NY - 2 && zp >= 1 && zp <= g.NZ - 2;
-                }
-                float ps;
-                if (pull && own_row) {  // uniform per warp: a warp covers part of one row
-                    m = pull_moments<C, kPeriodic>(g, codec, xn, yn, zn);
-                    have = true;
-                    ps = psi_of(m.rr, m.rb);
-                } else if (pull) {
-                    float rr, rb;
-                    pull_densities<C, kPeriodic>(g, codec, xn, yn, zn, rr, rb);
-                    ps = psi_of(rr, rb);
-                } else {
-                    ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
-                }
-                ringp[r * tpr + x] = ps;
-                if (own_row && xin) {
-                    float *q = msmp + (r - 1) * kMomCount * tpr + x;
-                    q[kMomRR * tpr] = m.rr;
-                    q[kMomRB * tpr] = m.rb;
-                    q[kMomUX * tpr] = m.ux;
-                    q[kMomUY * tpr] = m.uy;
-                    q[kMomUZ * tpr] = m.uz;
-                    q[kMomPXX * tpr] = m.pxx;
-                    q[kMomPXY * tpr] = m.pxy;
-                    q[kMomPYY * tpr] = m.pyy;
-                    q[kMomPYZ * tpr] = m.pyz;
-                    q[kMomPZZ * tpr] = m.pzz;
-                    q[kMomPXZ * tpr] = m.pxz;
-                    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
-                        // fluid-plane moments for the boundary launch
-                        float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
-                        const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy,
-                                                    m.pyz, m.pzz, m.pxz};
-#pragma unroll
-                        for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
-                    }
-                    if (std::is_same<C, CodecF32>::value && kPeriodic && s.tape) {
-                        // moment record of the pulled state (the adjoint sweep reads it)
-                        float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
-                        const size_t N = g.N;
-                        const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy,
-                                                      m.pyz, m.pzz, m.pxz, ps};
-#pragma unroll
-                        for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
-                    }
-                }
-            }
-            if constexpr (kStats) {
-                if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
-            }
+            tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
+                                            ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
         }
         if (T.cluster > 1) {
             // own rows of plane zp are now visible cluster-wide; copy the
@@ -604,26 +643,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
             const float *mc = msm + (zc & 1) * mplane;
             for (int r = 1 + lr; r <= ty; r += rpt) {
                 if (!xin) continue;
-                const int y = y0 - 1 + r;
-                const float *q = mc + (r - 1) * kMomCount * tpr + x;
-                NodeMoments m;
-                m.rr = q[kMomRR * tpr];
-                m.rb = q[kMomRB * tpr];
-                m.ux = q[kMomUX * tpr];
-                m.uy = q[kMomUY * tpr];
-                m.uz = q[kMomUZ * tpr];
-                m.pxx = q[kMomPXX * tpr];
-                m.pxy = q[kMomPXY * tpr];
-                m.pyy = q[kMomPYY * tpr];
-                m.pyz = q[kMomPYZ * tpr];
-                m.pzz = q[kMomPZZ * tpr];
-                m.pxz = q[kMomPXZ * tpr];
-                const int base = r * tpr + x;
-                auto psi_at = [&](int cx, int cy, int cz) {
-                    const float *pl = cz < 0 ? pm : (cz > 0 ? pp : p0);
-                    return pl[base + cy * tpr + cx];
-                };
-                collide_node(g, s.ph, codec, pop_row(g, y, zc), x, y, zc, m, psi_at);
+                tile_collide(s, codec, x, y0 - 1 + r, zc, r, mc + (r - 1) * kMomCount * tpr, pm, p0, pp, tpr);
             }
         }
         __syncthreads();
@@ -1525,6 +1545,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     t.tpr = ((g.NX + 31) / 32) * 32;
     const int per_row = t.tpr * 4;
     const int rpt = kFusedThreads / t.tpr;
+    if (const char *v = std::getenv("MCG_FUSED_SMEM_KB")) max_smem = std::atoi(v) * 1024;  // tuning sweeps
     // rows per tile: at least one round of rows in parallel, 4 by default
     // (measured best on 128x256x128), fewer if shared memory
     // (3*(ty+2) + 2*11*ty) * tpr * 4 bytes does not fit
@@ -1542,6 +1563,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
         const int c = std::atoi(v);
         if (c >= 1 && c <= 8 && t.ny_tiles % c == 0) t.cluster = c;
     }
+
     // z chunks: about seven CTAs per SM over the launch (measured best: 8-plane
     // chunks, 1024 CTAs on 128x256x128)
     const int target = 7 * 148;
