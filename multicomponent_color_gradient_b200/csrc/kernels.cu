@@ -46,6 +46,7 @@ constexpr unsigned kFull = 0xffffffffu;
 struct CodecF32 {
     using Elem = float;
     static constexpr int kGroupSlots = 6;
+    static constexpr bool kSumDiff = false;  // pulls form sum fr and sum fb (reference order)
     const float *__restrict__ rd;
     float *__restrict__ wr;
     int NX;
@@ -54,6 +55,13 @@ struct CodecF32 {
     __device__ __forceinline__ void store_row(float *wrow, float r, float b) const {
         wrow[slot_f32(I, 0) * NX] = r;
         wrow[slot_f32(I, 1) * NX] = b;
+    }
+    // bulk node: fr_i = aR w_i P_i, fb_i = aB w_i P_i (lbm.cuh:216-247)
+    __device__ __forceinline__ void store_bulk(float *wrow, float aR, float aB, const float (&P)[kQ]) const {
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            store_row<i>(wrow, (aR * Dir<i>::w) * P[i], (aB * Dir<i>::w) * P[i]);
+        });
     }
     // pull: `grow` = offset of the source row's group segment
     template <int I>
@@ -104,6 +112,7 @@ __device__ __forceinline__ void f16_decode(__half2 h, float w, float rho0, float
 struct CodecF16 {
     using Elem = __half2;
     static constexpr int kGroupSlots = 3;
+    static constexpr bool kSumDiff = true;  // pulls form sum (fr+fb) and sum (fr-fb)
     const __half2 *__restrict__ rd;
     __half2 *__restrict__ wr;
     int NX;
@@ -112,10 +121,31 @@ struct CodecF16 {
     __device__ __forceinline__ void store_row(__half2 *wrow, float r, float b) const {
         wrow[slot_f16(I) * NX] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
     }
+    // bulk node: every direction splits its total g_i = w_i P_i in the same
+    // proportion aR : aB, so the word is (P_i - rho0, q) with one signed
+    // minority fraction q = 2 min(aR, aB) for the node - the value f16_encode
+    // forms from fr_i, fb_i up to float rounding, and exactly +-0 at a pure
+    // node (aB or aR is exactly 0 there).
+    __device__ __forceinline__ void store_bulk(__half2 *wrow, float aR, float aB, const float (&P)[kQ]) const {
+        const float q = copysignf(fmaxf(2.0f * fminf(aR, aB), 0.0f), aR - aB);
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            wrow[slot_f16(i) * NX] = __floats2half2_rn(P[i] - rho0, q);
+        });
+    }
     template <int I>
     __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
         const __half2 h = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
         f16_decode(h, Dir<I>::w, rho0, r, b);
+    }
+    // total g = fr + fb and difference d = fr - fb of a word: with q the signed
+    // minority fraction, fr - fb = g (1 - q) when red is the majority and
+    // -g (1 + q) otherwise, i.e. g (sign(q) - q)
+    template <int I>
+    __device__ __forceinline__ void load_sd(size_t grow, int xs, float &gs, float &d) const {
+        const float2 v = __half22float2(__ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs));
+        gs = fmaf(Dir<I>::w, v.x, Dir<I>::w * rho0);
+        d = gs * (copysignf(1.0f, v.y) - v.y);
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
@@ -250,19 +280,27 @@ template <class C, bool kPeriodic>
 __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec, int x, int y, int z, float &rr,
                                                float &rb) {
     const PullMap<C> pm(g, x, y, z, kPeriodic);
-    float sumr = 0.f, sumb = 0.f;
+    float sumr = 0.f, sumb = 0.f;  // C::kSumDiff: sum (fr+fb) and sum (fr-fb)
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         size_t grow;
         int xs;
         pm.template src<i>(x, grow, xs);
-        float fr, fb;
-        codec.template load<i>(grow, xs, fr, fb);
-        sumr += fr;
-        sumb += fb;
+        float u, v;
+        if constexpr (C::kSumDiff)
+            codec.template load_sd<i>(grow, xs, u, v);
+        else
+            codec.template load<i>(grow, xs, u, v);
+        sumr += u;
+        sumb += v;
     });
-    rr = sumr;
-    rb = sumb;
+    if constexpr (C::kSumDiff) {
+        rr = 0.5f * (sumr + sumb);
+        rb = 0.5f * (sumr - sumb);
+    } else {
+        rr = sumr;
+        rb = sumb;
+    }
 }
 
 // Pull the 54 populations of interior node (x,y,z) and form its moments
@@ -270,7 +308,7 @@ __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec
 template <class C, bool kPeriodic>
 __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &codec, int x, int y, int z) {
     const PullMap<C> pm(g, x, y, z, kPeriodic);
-    float sumr = 0.f, sumb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+    float sumr = 0.f, sumb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;  // C::kSumDiff: sum (fr+fb), sum (fr-fb)
     float Axx = 0.f, Axy = 0.f, Ayy = 0.f, Ayz = 0.f, Azz = 0.f, Axz = 0.f;
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
@@ -278,11 +316,19 @@ __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &
         size_t grow;
         int xs;
         pm.template src<i>(x, grow, xs);
-        float fr, fb;
-        codec.template load<i>(grow, xs, fr, fb);
-        sumr += fr;
-        sumb += fb;
-        const float gi = fr + fb;
+        float gi;
+        if constexpr (C::kSumDiff) {
+            float d;
+            codec.template load_sd<i>(grow, xs, gi, d);
+            sumr += gi;
+            sumb += d;
+        } else {
+            float fr, fb;
+            codec.template load<i>(grow, xs, fr, fb);
+            sumr += fr;
+            sumb += fb;
+            gi = fr + fb;
+        }
         if constexpr (D::cx == 1) jx += gi;
         if constexpr (D::cx == -1) jx -= gi;
         if constexpr (D::cy == 1) jy += gi;
@@ -296,6 +342,11 @@ __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &
         Azz += gi * D::Hzz;
         if constexpr (D::Hxz != 0.0f) Axz += gi * D::Hxz;
     });
+    if constexpr (C::kSumDiff) {
+        const float sg = sumr, sd = sumb;
+        sumr = 0.5f * (sg + sd);
+        sumb = 0.5f * (sg - sd);
+    }
     NodeMoments m;
     const float rho = sumr + sumb;
     const float inv = 1.0f / rho;
@@ -334,10 +385,7 @@ __device__ __forceinline__ void collide_node(const Geometry &g, const Physics &p
     collision_poly(rT, m.ux, m.uy, m.uz, n, oms, P);
     typename C::Elem *const wrow = codec.wr + row + x;
     if (Iind <= 1e-4f) {  // bulk (lbm.cuh:216-247)
-        static_for<kQ>([&](auto I) {
-            constexpr int i = decltype(I)::value;
-            codec.template store_row<i>(wrow, (aR * Dir<i>::w) * P[i], (aB * Dir<i>::w) * P[i]);
-        });
+        codec.store_bulk(wrow, aR, aB, P);
         return;
     }
     // interface (lbm.cuh:249-292): colour gradient over the 26 neighbours
