@@ -60,7 +60,9 @@ struct CodecF32 {
     __device__ __forceinline__ void store_bulk(float *wrow, float aR, float aB, const float (&P)[kQ]) const {
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            store_row<i>(wrow, (aR * Dir<i>::w) * P[i], (aB * Dir<i>::w) * P[i]);
+            // both colours in one packed multiply
+            const float2 f = __fmul2_rn(make_float2(aR * Dir<i>::w, aB * Dir<i>::w), make_float2(P[i], P[i]));
+            store_row<i>(wrow, f.x, f.y);
         });
     }
     // pull: `grow` = offset of the source row's group segment
@@ -145,7 +147,7 @@ struct CodecF16 {
     __device__ __forceinline__ void load_sd(size_t grow, int xs, float &gs, float &d) const {
         const float2 v = __half22float2(__ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs));
         gs = fmaf(Dir<I>::w, v.x, Dir<I>::w * rho0);
-        d = gs * (copysignf(1.0f, v.y) - v.y);
+        d = fmaf(-gs, v.y, copysignf(gs, v.y));
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
@@ -280,7 +282,7 @@ template <class C, bool kPeriodic>
 __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec, int x, int y, int z, float &rr,
                                                float &rb) {
     const PullMap<C> pm(g, x, y, z, kPeriodic);
-    float sumr = 0.f, sumb = 0.f;  // C::kSumDiff: sum (fr+fb) and sum (fr-fb)
+    float2 sum = make_float2(0.f, 0.f);  // (sum fr, sum fb); C::kSumDiff: (sum fr+fb, sum fr-fb)
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         size_t grow;
@@ -291,15 +293,14 @@ __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec
             codec.template load_sd<i>(grow, xs, u, v);
         else
             codec.template load<i>(grow, xs, u, v);
-        sumr += u;
-        sumb += v;
+        sum = __fadd2_rn(sum, make_float2(u, v));  // both colours in one packed add
     });
     if constexpr (C::kSumDiff) {
-        rr = 0.5f * (sumr + sumb);
-        rb = 0.5f * (sumr - sumb);
+        rr = 0.5f * (sum.x + sum.y);
+        rb = 0.5f * (sum.x - sum.y);
     } else {
-        rr = sumr;
-        rb = sumb;
+        rr = sum.x;
+        rb = sum.y;
     }
 }
 
@@ -308,7 +309,8 @@ __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec
 template <class C, bool kPeriodic>
 __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &codec, int x, int y, int z) {
     const PullMap<C> pm(g, x, y, z, kPeriodic);
-    float sumr = 0.f, sumb = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;  // C::kSumDiff: sum (fr+fb), sum (fr-fb)
+    float2 sum = make_float2(0.f, 0.f);  // (sum fr, sum fb); C::kSumDiff: (sum fr+fb, sum fr-fb)
+    float jx = 0.f, jy = 0.f, jz = 0.f;
     float Axx = 0.f, Axy = 0.f, Ayy = 0.f, Ayz = 0.f, Azz = 0.f, Axz = 0.f;
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
@@ -320,13 +322,11 @@ __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &
         if constexpr (C::kSumDiff) {
             float d;
             codec.template load_sd<i>(grow, xs, gi, d);
-            sumr += gi;
-            sumb += d;
+            sum = __fadd2_rn(sum, make_float2(gi, d));
         } else {
             float fr, fb;
             codec.template load<i>(grow, xs, fr, fb);
-            sumr += fr;
-            sumb += fb;
+            sum = __fadd2_rn(sum, make_float2(fr, fb));
             gi = fr + fb;
         }
         if constexpr (D::cx == 1) jx += gi;
@@ -342,10 +342,10 @@ __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &
         Azz += gi * D::Hzz;
         if constexpr (D::Hxz != 0.0f) Axz += gi * D::Hxz;
     });
+    float sumr = sum.x, sumb = sum.y;
     if constexpr (C::kSumDiff) {
-        const float sg = sumr, sd = sumb;
-        sumr = 0.5f * (sg + sd);
-        sumb = 0.5f * (sg - sd);
+        sumr = 0.5f * (sum.x + sum.y);
+        sumb = 0.5f * (sum.x - sum.y);
     }
     NodeMoments m;
     const float rho = sumr + sumb;
