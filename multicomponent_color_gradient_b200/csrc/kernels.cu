@@ -438,7 +438,7 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
     const Physics &ph = s.ph;
     const int lane = threadIdx.x & 31;
     unsigned key = 0xffffffffu;
-    double v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0;
+    float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f, v4 = 0.f;
     if (active) {
         const float dx = float(x) - ph.jet_x0, dz = float(z) - ph.jet_z0;
         const float r = sqrtf(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)));
@@ -447,23 +447,24 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
             key = (rb << 1) | (dx < 0.0f ? 1u : 0u);
             float ur = 0.0f;
             if (r > 1.0e-12f) ur = (ux * dx + uz * dz) / r;
-            const double duy = double(uy), dur = double(ur);
-            v0 = duy;
-            v1 = duy * duy;
-            v2 = dur;
-            v3 = dur * dur;
-            v4 = dur * duy;
+            v0 = uy;
+            v1 = uy * uy;
+            v2 = ur;
+            v3 = ur * ur;
+            v4 = ur * uy;
         }
     }
     if (__all_sync(kFull, key == 0xffffffffu)) return;
+    // run sums in float32 (a run is at most 32 nodes of one row); the run
+    // totals go into the float64 accumulators
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const unsigned ok = __shfl_up_sync(kFull, key, d);
-        const double o0 = __shfl_up_sync(kFull, v0, d);
-        const double o1 = __shfl_up_sync(kFull, v1, d);
-        const double o2 = __shfl_up_sync(kFull, v2, d);
-        const double o3 = __shfl_up_sync(kFull, v3, d);
-        const double o4 = __shfl_up_sync(kFull, v4, d);
+        const float o0 = __shfl_up_sync(kFull, v0, d);
+        const float o1 = __shfl_up_sync(kFull, v1, d);
+        const float o2 = __shfl_up_sync(kFull, v2, d);
+        const float o3 = __shfl_up_sync(kFull, v3, d);
+        const float o4 = __shfl_up_sync(kFull, v4, d);
         if (lane >= d && ok == key) {
             v0 += o0; v1 += o1; v2 += o2; v3 += o3; v4 += o4;
         }
@@ -473,11 +474,11 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
     if (tail && key != 0xffffffffu) {
         const size_t M = size_t(s.g.NY) * ph.NRB;
         const size_t mi = size_t(y) * ph.NRB + (key >> 1);
-        atomicAdd(s.radial + mi, v0);
-        atomicAdd(s.radial + M + mi, v1);
-        atomicAdd(s.radial + 2 * M + mi, v2);
-        atomicAdd(s.radial + 3 * M + mi, v3);
-        atomicAdd(s.radial + 4 * M + mi, v4);
+        atomicAdd(s.radial + mi, double(v0));
+        atomicAdd(s.radial + M + mi, double(v1));
+        atomicAdd(s.radial + 2 * M + mi, double(v2));
+        atomicAdd(s.radial + 3 * M + mi, double(v3));
+        atomicAdd(s.radial + 4 * M + mi, double(v4));
     }
 }
 
