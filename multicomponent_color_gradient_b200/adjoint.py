@@ -34,6 +34,8 @@ class FourierModes:
         self.NX, self.NY, self.NZ = int(c["NX"]), int(c["NY"]), int(c["NZ"])
         self.N = self.NX * self.NY * self.NZ
         L = np.array([self.NX - 2, self.NY - 2, self.NZ - 2], np.float64)
+        if not 2 * max_mode < L.min():
+            raise ValueError("max_mode must be below half the interior extent")
         waves = []
         rng = range(-max_mode, max_mode + 1)
         for nz in rng:
@@ -63,26 +65,41 @@ class FourierModes:
         self.e = np.array(pols)        # (M, 3)
         self.phase = np.array(phases)  # (M,)
         self.count = len(phases)
-        z, y, x = np.meshgrid(np.arange(self.NZ), np.arange(self.NY), np.arange(self.NX), indexing="ij")
-        self._interior = ((x >= 1) & (x <= self.NX - 2) & (y >= 1) & (y <= self.NY - 2) & (z >= 1) &
-                          (z <= self.NZ - 2)).reshape(-1)
-        xi = np.stack([(x - 1).reshape(-1), (y - 1).reshape(-1), (z - 1).reshape(-1)], 1).astype(np.float64)
-        self._xi = xi[self._interior]  # (Nint, 3)
+        self.n = np.array([w for w in waves for _ in (0, 1)], np.int64)  # (M, 3) integer wave vectors
+        self.L = L.astype(np.int64)
 
-    def _cos(self) -> np.ndarray:
-        return np.cos(self._xi @ self.k.T + self.phase[None, :])  # (Nint, M)
+    # Synthesis and projection run through FFTs of the interior: mode m puts
+    # a_m e_m exp(i phi_m) at wave vector n_m of the spectrum A, and
+    # u = Re sum_n A_n exp(i k_n . xi) is L^3 times the real part of the
+    # inverse FFT.  The projection is the transpose: Re(exp(i phi_m) e_m .
+    # conj(V(n_m))) with V the forward FFT of the field.
+
+    def _spectral_index(self):
+        Lx, Ly, Lz = self.L
+        return self.n[:, 2] % Lz, self.n[:, 1] % Ly, self.n[:, 0] % Lx
 
     def velocity(self, a: np.ndarray) -> np.ndarray:
-        """u0 as (3, Ncells) float64 from amplitudes a (M,)."""
+        """u0 as (3, Ncells) float64 from amplitudes a (M,); ghost nodes 0."""
         a = np.asarray(a, np.float64).reshape(self.count)
-        u = np.zeros((3, self.N))
-        u[:, self._interior] = ((self._cos() * a[None, :]) @ self.e).T
-        return u
+        Lx, Ly, Lz = self.L
+        iz, iy, ix = self._spectral_index()
+        coef = a * np.exp(1j * self.phase)
+        u = np.zeros((3, self.NZ, self.NY, self.NX))
+        for c in range(3):
+            A = np.zeros((Lz, Ly, Lx), np.complex128)
+            np.add.at(A, (iz, iy, ix), coef * self.e[:, c])
+            u[c, 1:-1, 1:-1, 1:-1] = np.fft.ifftn(A).real * (Lx * Ly * Lz)
+        return u.reshape(3, self.N)
 
     def project(self, v: np.ndarray) -> np.ndarray:
         """The transpose of ``velocity``: sum_x v(x) . e_m cos(k_m.x + phi_m)."""
-        v = np.asarray(v, np.float64).reshape(3, self.N)[:, self._interior]
-        return np.einsum("nm,mc,cn->m", self._cos(), self.e, v)
+        v = np.asarray(v, np.float64).reshape(3, self.NZ, self.NY, self.NX)[:, 1:-1, 1:-1, 1:-1]
+        iz, iy, ix = self._spectral_index()
+        out = np.zeros(self.count)
+        for c in range(3):
+            V = np.fft.fftn(v[c])
+            out += self.e[:, c] * np.real(np.exp(1j * self.phase) * np.conj(V[iz, iy, ix]))
+        return out
 
 
 class BubbleProblem:

@@ -46,6 +46,16 @@ def test_schedule_depth_is_binomial():
         assert f == r * (T + 1) - comb(snaps + r, snaps + 1)
 
 
+def dense_velocity(M, a):
+    """Direct sum of the modes at every interior node (small grids only)."""
+    z, y, x = np.meshgrid(np.arange(M.NZ), np.arange(M.NY), np.arange(M.NX), indexing="ij")
+    xi = np.stack([(x - 1).ravel(), (y - 1).ravel(), (z - 1).ravel()], 1).astype(np.float64)
+    inside = ((x >= 1) & (x <= M.NX - 2) & (y >= 1) & (y <= M.NY - 2) & (z >= 1) & (z <= M.NZ - 2)).ravel()
+    u = np.zeros((3, M.N))
+    u[:, inside] = ((np.cos(xi[inside] @ M.k.T + M.phase[None, :]) * a[None, :]) @ M.e).T
+    return u
+
+
 def test_fourier_modes_are_divergence_free_and_project_is_the_transpose():
     case = get_case("adjoint_bubble_96", NX=14, NY=12, NZ=10)
     M = FourierModes(case, max_mode=1, seed=5)
@@ -53,17 +63,28 @@ def test_fourier_modes_are_divergence_free_and_project_is_the_transpose():
     assert np.allclose(np.einsum("mc,mc->m", M.k, M.e), 0.0)
     rng = np.random.default_rng(0)
     a = rng.normal(size=M.count)
+    # the FFT synthesis equals the direct sum of the modes
+    np.testing.assert_allclose(M.velocity(a), dense_velocity(M, a), atol=1e-12)
     v = rng.normal(size=(3, M.N))
     lhs = float(np.sum(M.velocity(a) * v))
     rhs = float(a @ M.project(v))
     assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
     u = M.velocity(a).reshape(3, 10, 12, 14)
     assert np.all(u[:, 0] == 0) and np.all(u[:, :, :, -1] == 0)
-    # periodic over the interior: the field at x = 1 continues the one at x = NX - 2
-    ux = u[0, 1:-1, 1:-1, 1:-1]
-    L = 12
-    xi = np.arange(L + 1)
-    k = M.k[:, 0]
-    val = np.cos(np.outer(xi, k) + M.phase[None, :]) @ (a * M.e[:, 0])
-    assert np.allclose(val[0], val[L])
-    assert np.allclose(ux[0, 0, :], val[:L])
+
+
+def test_fourier_modes_eight_per_axis():
+    """8 modes per axis on a 22^3 interior: 2456 wave vectors, 4912 amplitudes;
+    the spectral divergence k . e vanishes and synthesis/projection stay adjoint."""
+    case = get_case("adjoint_bubble_96", NX=24, NY=24, NZ=24)
+    M = FourierModes(case, max_mode=8, seed=2)
+    assert M.count == 2 * (17 ** 3 - 1) // 2
+    assert np.allclose(np.einsum("mc,mc->m", M.k, M.e), 0.0, atol=1e-12)
+    rng = np.random.default_rng(3)
+    a = rng.normal(size=M.count) * 1e-3
+    v = rng.normal(size=(3, M.N))
+    lhs = float(np.sum(M.velocity(a) * v))
+    rhs = float(a @ M.project(v))
+    assert abs(lhs - rhs) <= 1e-9 * abs(lhs)
+    with pytest.raises(ValueError):
+        FourierModes(case, max_mode=11)
