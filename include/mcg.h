@@ -242,6 +242,20 @@ mcg_status mcg_check_finite(mcg_handle *h);
 mcg_status mcg_conservation_sums_static(const float *fr, const float *fb, int32_t NX, int32_t NY, int32_t NZ,
                                         double *out5, void *stream);
 
+/* ---------------- inlet profile (no counterpart in the reference) ---------------- */
+
+#define MCG_INLET_BESSEL_MAX 8
+/* Radial inlet profile around the top-hat: in jet columns the inlet velocity
+ * U of jet/boundary_conditions.cuh:62 becomes U m(r) with
+ *   m(r) = 1 + sum_{k=1..n} c_k J0(alpha_k r / R),
+ * alpha_k the k-th zero of J0, r the distance of the column from the jet axis
+ * (as in the inlet mask, utilities/mathUtilities.cuh:14-21), R = jet_radius.
+ * n = 0 restores the top-hat (the reference's profile); n <= MCG_INLET_BESSEL_MAX.
+ * The seeded perturbation (inlet_noise) multiplies on top. */
+mcg_status mcg_set_inlet_bessel(mcg_handle *h, const float *coeffs, int32_t n);
+/* The per-column multipliers m (NX*NZ floats, x fastest; 1 everywhere for the top-hat). */
+mcg_status mcg_get_inlet_profile(mcg_handle *h, float *profile);
+
 /* ---------------- discrete adjoint (no counterpart in the reference) ---------------- */
 
 /* Initial state with a velocity field: every interior node gets, per colour,

@@ -90,6 +90,8 @@ SIGNATURES = {
     "mcg_check_finite": [_P],
     "mcg_conservation_sums_static": [_P, _P, C.c_int32, C.c_int32, C.c_int32, _P, _P],
     "mcg_init_equilibrium": [_P, _F, _F, _F, _F, _F],
+    "mcg_set_inlet_bessel": [_P, _F, C.c_int32],
+    "mcg_get_inlet_profile": [_P, _F],
     "mcg_adjoint_run": [_P, _F, C.c_int32, C.c_int32, _D, _D, _D, _F, C.POINTER(C.c_int64), _F],
     "mcg_adjoint_plan": [C.c_int32, C.c_int32, C.POINTER(C.c_int64), _I32],
     "mcg_output_open": [_P, C.c_char_p],

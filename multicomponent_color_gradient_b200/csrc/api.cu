@@ -139,8 +139,8 @@ size_t pop_buffer_bytes(const mcg_params &p) {
 
 void release(mcg_handle *h) {
     mcg::io_close(h);
-    void *ptrs[] = {h->s.pops[0], h->s.pops[1], h->s.mom, h->s.psi[0], h->s.psi[1],
-                    h->s.radial,  h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar, h->s.bmom};
+    void *ptrs[] = {h->s.pops[0], h->s.pops[1], h->s.mom,      h->s.psi[0], h->s.psi[1], h->s.radial,
+                    h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar, h->s.bmom,  h->d_inlet_profile};
     for (void *q : ptrs)
         if (q) cudaFree(q);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
@@ -424,6 +424,73 @@ mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *r
     if (mcg_status s = mcg_set_fields(h, rhor, rhob, ux, uy, uz)) return s;
     MCG_LAUNCH(h, mcg::launch_init_pops(h->s, 3, nullptr, nullptr, 0.0f, h->stream), "equilibrium populations");
     MCG_CUDA(cudaStreamSynchronize(h->stream), "init equilibrium");
+    return MCG_OK;
+}
+
+// ---------------------------------------------------------------- inlet profile
+
+namespace {
+// k-th positive zero of J0 (k >= 1): Newton's method on J0 (derivative -J1)
+// from McMahon's asymptotic estimate (k - 1/4) pi.
+double bessel_j0_zero(int k) {
+    double x = (double(k) - 0.25) * M_PI;
+    for (int it = 0; it < 60; ++it) {
+        const double dx = std::cyl_bessel_j(0.0, x) / -std::cyl_bessel_j(1.0, x);
+        x -= dx;
+        if (std::fabs(dx) < 1e-15 * x) break;
+    }
+    return x;
+}
+}  // namespace
+
+mcg_status mcg_set_inlet_bessel(mcg_handle *h, const float *coeffs, int32_t n) {
+    if (mcg_status s = check_handle(h)) return s;
+    MCG_REQUIRE(n >= 0 && n <= MCG_INLET_BESSEL_MAX, "n must be in [0, MCG_INLET_BESSEL_MAX]");
+    MCG_REQUIRE(n == 0 || coeffs != nullptr, "coeffs is null");
+    for (int k = 0; k < n; ++k) MCG_REQUIRE(std::isfinite(coeffs[k]), "coefficients must be finite");
+    const mcg_params &p = h->p;
+    if (n == 0) {  // back to the top-hat
+        h->s.inlet_profile = nullptr;
+        h->inlet_coeffs.clear();
+        return MCG_OK;
+    }
+    // multiplier m(r) = 1 + sum_k c_k J0(alpha_k r / R) of every column, with r
+    // measured from the jet axis like the inlet mask (mathUtilities.cuh:14-21)
+    const int NX = p.NX, NZ = p.NZ;
+    std::vector<double> alpha(static_cast<size_t>(n));
+    for (int k = 0; k < n; ++k) alpha[size_t(k)] = bessel_j0_zero(k + 1);
+    std::vector<float> prof(size_t(NX) * NZ);
+    const double R = p.jet_radius;
+    for (int z = 0; z < NZ; ++z)
+        for (int x = 0; x < NX; ++x) {
+            const double dx = double(float(x) - p.jet_x0), dz = double(float(z) - p.jet_z0);
+            const double r = std::sqrt(dx * dx + dz * dz);
+            double m = 1.0;
+            for (int k = 0; k < n; ++k) m += double(coeffs[k]) * std::cyl_bessel_j(0.0, alpha[size_t(k)] * r / R);
+            prof[size_t(z) * NX + x] = float(m);
+        }
+    if (!h->d_inlet_profile)
+        MCG_CUDA(cudaMalloc(&h->d_inlet_profile, prof.size() * sizeof(float)), "inlet profile allocation");
+    MCG_CUDA(cudaMemcpyAsync(h->d_inlet_profile, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice,
+                             h->stream),
+             "upload inlet profile");
+    MCG_CUDA(cudaStreamSynchronize(h->stream), "inlet profile");
+    h->s.inlet_profile = h->d_inlet_profile;
+    h->inlet_coeffs.assign(coeffs, coeffs + n);
+    return MCG_OK;
+}
+
+mcg_status mcg_get_inlet_profile(mcg_handle *h, float *profile) {
+    if (mcg_status s = check_handle(h)) return s;
+    MCG_REQUIRE(profile != nullptr, "profile is null");
+    const size_t n = size_t(h->p.NX) * h->p.NZ;
+    if (!h->s.inlet_profile) {
+        for (size_t i = 0; i < n; ++i) profile[i] = 1.0f;
+        return MCG_OK;
+    }
+    MCG_CUDA(cudaMemcpyAsync(profile, h->s.inlet_profile, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+             "download inlet profile");
+    MCG_CUDA(cudaStreamSynchronize(h->stream), "inlet profile");
     return MCG_OK;
 }
 

@@ -35,6 +35,8 @@ struct mcg_handle {
     float tke_total = 0.f, tke_avg = 0.f, tke_avg_prev = 0.f, tke_delta = 0.f, tke_abs_delta = 0.f;
     uint32_t uy_avg_samples = 0;
 
+    float *d_inlet_profile = nullptr;   // [NZ][NX] inlet velocity multipliers (mcg_set_inlet_bessel)
+    std::vector<float> inlet_coeffs;    // the Bessel coefficients it was made from
     double *d_scalar = nullptr;  // 8 doubles of device scratch for reductions
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> prof_events;  // mcg_step_profiled

@@ -194,10 +194,16 @@ __device__ __forceinline__ bool is_jet_column(const Physics &ph, int x, int z) {
     return dx * dx + dz * dz <= ph.jet_r2;
 }
 
-__device__ __forceinline__ float inlet_velocity(const Physics &ph, int64_t step, int x, int z) {
-    if (ph.inlet_noise == 0.0f) return ph.jet_velocity;
+// Inlet velocity of jet column (x, z): the top-hat U (boundary_conditions.cuh:62),
+// times the column's profile multiplier when a radial profile is set, times
+// the seeded perturbation when inlet_noise != 0.
+__device__ __forceinline__ float inlet_velocity(const DeviceState &s, int64_t step, int x, int z) {
+    const Physics &ph = s.ph;
+    float U = ph.jet_velocity;
+    if (s.inlet_profile) U *= s.inlet_profile[x + s.g.NX * z];
+    if (ph.inlet_noise == 0.0f) return U;
     const float u = hash_uniform(ph.seed, 0x1A1E7ull ^ uint64_t(step), uint64_t(x), uint64_t(z));
-    return ph.jet_velocity * (1.0f + (2.0f * u - 1.0f) * ph.inlet_noise);
+    return U * (1.0f + (2.0f * u - 1.0f) * ph.inlet_noise);
 }
 
 __host__ __device__ __forceinline__ int wrap_interior(int v, int n) { return v == 0 ? n - 2 : (v == n - 1 ? 1 : v); }
@@ -795,7 +801,7 @@ __device__ __forceinline__ void inlet_column(const DeviceState &s, void *dst, fl
     const float rT = rrB + rbB;
     const float aR = rrB * (1.0f / rT), aB = rbB * (1.0f / rT);
     const float oms = 1.0f - ph.omega_b;
-    const EqTerms e = make_eq(0.0f, inlet_velocity(ph, step, x, z), 0.0f);
+    const EqTerms e = make_eq(0.0f, inlet_velocity(s, step, x, z), 0.0f);
     const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;

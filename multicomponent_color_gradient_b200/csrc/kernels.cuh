@@ -99,6 +99,7 @@ struct DeviceState {
     uint32_t partials_cap;
     int *flag;        // device flag (non-finite detection)
     float *tape;      // null, or [kTapePlanes][N]: the fused step records the moments and psi it pulls there
+    const float *inlet_profile;  // null (top-hat), or [NZ][NX] multipliers of the inlet velocity per column
 };
 
 // ---- the fused step (moments + colour gradient + collision in one pass) ----

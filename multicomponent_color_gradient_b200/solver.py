@@ -114,6 +114,19 @@ class Solver:
         assert all(a.size == self.N for a in arrs)
         self._c("mcg_init_equilibrium", *[_fptr(a) for a in arrs])
 
+    # -- inlet profile ---------------------------------------------------------
+    def set_inlet_bessel(self, coeffs) -> None:
+        """Inlet velocity U (1 + sum_k c_k J0(alpha_k r / R)) in jet columns
+        (alpha_k the zeros of J0); an empty sequence restores the top-hat."""
+        c = np.ascontiguousarray(coeffs, dtype=np.float32).reshape(-1)
+        self._c("mcg_set_inlet_bessel", _fptr(c) if c.size else None, int(c.size))
+
+    def inlet_profile(self) -> np.ndarray:
+        """Per-column inlet velocity multipliers, (NZ, NX)."""
+        out = np.empty(self.case["NX"] * self.case["NZ"], np.float32)
+        self._c("mcg_get_inlet_profile", _fptr(out))
+        return out.reshape(self.case["NZ"], self.case["NX"])
+
     # -- discrete adjoint (periodic box, float32 storage) ----------------------
     def adjoint_run(self, psi_target, nsteps: int, snapshots: int) -> Dict:
         """J = sum (psi_T - psi_target)^2 over interior nodes after `nsteps`

@@ -116,6 +116,7 @@ struct Oracle {
     std::vector<double> s_uy, s_uy2, s_ur, s_ur2, s_uruy;
     std::vector<uint64_t> cnt;
     std::vector<T> uy_avg;
+    std::vector<T> inlet_prof;  // per-column inlet velocity multipliers (empty: top-hat)
     uint32_t uy_avg_count = 0;
     T tke_total = 0, tke_avg = 0;
     int64_t step = 0;
@@ -390,12 +391,16 @@ struct Oracle {
                 }
     }
 
-    // Seeded inlet-velocity factor (extension; 1 when inlet_noise == 0).
+    // Inlet velocity of a jet column: the top-hat U, times the column's radial
+    // profile multiplier when one is set, times the seeded perturbation
+    // (extensions; U itself when neither is set).
     T inlet_uy(int x, int z) const {
-        if (p.inlet_noise == 0.0f) return jet_velocity;
+        T U = jet_velocity;
+        if (!inlet_prof.empty()) U = U * inlet_prof[size_t(z) * NX + x];
+        if (p.inlet_noise == 0.0f) return U;
         const float u = hash_uniform(p.seed, 0x1A1E7ull ^ uint64_t(step), uint64_t(x), uint64_t(z));
         const float f = 1.0f + (2.0f * u - 1.0f) * p.inlet_noise;
-        return jet_velocity * T(f);
+        return U * T(f);
     }
 
     // jet/boundary_conditions.cuh:17-85 over interior x,z (kernels.cu:98-114)
@@ -606,6 +611,11 @@ void orc_set_fields(void *hv, const double *rr, const double *rb, const double *
                     const double *vz) {
     Handle *h = static_cast<Handle *>(hv);
     DISPATCH(h, (copy_in(O.rhor, rr), copy_in(O.rhob, rb), copy_in(O.ux, vx), copy_in(O.uy, vy), copy_in(O.uz, vz)));
+}
+// Per-column inlet velocity multipliers (NX*NZ, x fastest); NULL restores the top-hat.
+void orc_set_inlet_profile(void *hv, const double *prof) {
+    Handle *h = static_cast<Handle *>(hv);
+    DISPATCH(h, (prof ? (O.inlet_prof.assign(prof, prof + size_t(O.NX) * O.NZ), 0) : (O.inlet_prof.clear(), 0)));
 }
 void orc_get_fields(void *hv, double *rr, double *rb, double *vx, double *vy, double *vz) {
     Handle *h = static_cast<Handle *>(hv);

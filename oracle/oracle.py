@@ -36,6 +36,7 @@ def _load():
         "orc_get_pops": ([P, D, D], None),
         "orc_set_fields": ([P, D, D, D, D, D], None),
         "orc_get_fields": ([P, D, D, D, D, D], None),
+        "orc_set_inlet_profile": ([P, D], None),
         "orc_get_stress": ([P, D], None),
         "orc_macros": ([P], None),
         "orc_collistream": ([P], None),
@@ -117,6 +118,15 @@ class Oracle:
     def set_fields(self, rhor, rhob, ux, uy, uz):
         arrs = [np.ascontiguousarray(a, np.float64).reshape(-1) for a in (rhor, rhob, ux, uy, uz)]
         self.lib.orc_set_fields(self._h, *[_dp(a) for a in arrs])
+
+    def set_inlet_profile(self, prof):
+        """Per-column inlet velocity multipliers ((NZ, NX) or NX*NZ); None restores the top-hat."""
+        if prof is None:
+            self.lib.orc_set_inlet_profile(self._h, None)
+            return
+        a = np.ascontiguousarray(prof, np.float64).reshape(-1)
+        assert a.size == self.NX * self.NZ
+        self.lib.orc_set_inlet_profile(self._h, _dp(a))
 
     def get_fields(self):
         out = {k: np.empty(self.N) for k in ("rhor", "rhob", "ux", "uy", "uz")}
