@@ -707,6 +707,73 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     if (T.cluster > 1) cluster.sync();
 }
 
+// ------------------------------------------------------------------ software-pipelined fused step
+
+// The tile march of k_fused with the pull and the relaxation in the same
+// phase: iteration k pulls march plane k and relaxes march plane k-2, whose
+// psi neighbours (planes k-3 .. k-1) and moments were pulled in earlier
+// iterations.  The pull writes ring slot k mod 4 and stage slot k mod 3; the
+// relaxation reads ring slots k-3 .. k-1 and stage slot k-2 - all different -
+// so one __syncthreads per iteration suffices.  Between barriers the warps of
+// a CTA drift apart, and the memory-bound pull of one warp overlaps the
+// ALU-bound relaxation of another.
+constexpr int kPipeRing = 4, kPipeStage = 3;
+#ifndef MCG_PIPE_MIN_BLOCKS
+#define MCG_PIPE_MIN_BLOCKS 2
+#endif
+
+template <class C, bool kStats, bool kPeriodic>
+__global__ void __launch_bounds__(kFusedThreads, MCG_PIPE_MIN_BLOCKS) k_fused_pipe(const DeviceState s,
+                                                                                  const FusedTiling T, int cur,
+                                                                                  int64_t step) {
+    extern __shared__ float sm[];
+    const Geometry &g = s.g;
+    const int tpr = T.tpr;
+    const int rpt = kFusedThreads / tpr;
+    const int lr0 = threadIdx.x / tpr;
+    const int lr = lr0 < rpt ? lr0 : T.ty + 2;  // idle groups (tpr not dividing the block) skip every row
+    const int x = threadIdx.x - lr0 * tpr;
+    const int y0 = 1 + int(blockIdx.x) * T.ty;
+    const int ty = min(T.ty, g.NY - 1 - y0);
+    const int z0 = 1 + int(blockIdx.y) * T.lz;
+    const int lz = min(T.lz, g.NZ - 1 - z0);
+    const int pstride = (T.ty + 2) * tpr;
+    const int mplane = T.ty * kMomCount * tpr;
+    float *ring = sm;                        // [4][ty+2][tpr]
+    float *msm = sm + kPipeRing * pstride;   // [3][ty][11][tpr]
+    const C codec = make_codec<C>(s, cur);
+    const float *__restrict__ psi_g = s.psi[step & 1];
+    const bool xin = x >= 1 && x <= g.NX - 2;
+    const bool down = T.alternate && (blockIdx.y & 1);
+    auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
+    for (int k = 0; k <= lz + 2; ++k) {
+        const bool do_pull = k <= lz + 1;
+        const int c = k - 2;  // march index of the plane relaxed in this iteration
+        const bool do_relax = c >= 1 && c <= lz;
+        const int zp = plane(k);
+        float *ringp = ring + (k % kPipeRing) * pstride;
+        float *msmp = msm + (k % kPipeStage) * mplane;
+        const bool own_plane = k >= 1 && k <= lz;
+        const int zc = plane(c);
+        const float *pm = ring + (((down ? c + 1 : c - 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc-1
+        const float *p0 = ring + ((c + kPipeRing) % kPipeRing) * pstride;                       // plane zc
+        const float *pp = ring + (((down ? c - 1 : c + 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc+1
+        const float *mc = msm + ((c + kPipeStage) % kPipeStage) * mplane;
+        // rows of this thread: pull rows lr, lr+rpt, ... (< ty+2) and relax rows
+        // 1+lr, 1+lr+rpt, ... (<= ty), interleaved so that a warp has loads of
+        // one row in flight while it relaxes another
+        for (int r = lr; r < ty + 2; r += rpt) {
+            if (do_pull)
+                tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
+                                                ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
+            const int rc = r + 1;
+            if (do_relax && rc <= ty && xin)
+                tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+        }
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------------ granular sequence
 
 constexpr int kBX = 32, kBY = 8;
@@ -1149,11 +1216,20 @@ unsigned grid1(const Geometry &g) {
 
 template <class C, bool kStats, bool kPeriodic>
 cudaError_t fused_attr(int smem) {
-    return cudaFuncSetAttribute(k_fused<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_fused<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fused_pipe<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem);
 }
 
 template <class C, bool kStats, bool kPeriodic>
 cudaError_t fused_launch(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
+    if (t.pipe) {
+        k_fused_pipe<C, kStats, kPeriodic>
+            <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
+        return cudaGetLastError();
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(t.ny_tiles, t.nz_chunks);
     cfg.blockDim = dim3(kFusedThreads);
@@ -1601,12 +1677,22 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     const int per_row = t.tpr * 4;
     const int rpt = kFusedThreads / t.tpr;
     if (const char *v = std::getenv("MCG_FUSED_SMEM_KB")) max_smem = std::atoi(v) * 1024;  // tuning sweeps
+    // software-pipelined march for float32 rows of up to 128 columns (4-row
+    // tiles at two CTAs per SM; measured +5 % on 128x256x128).  Float16 is
+    // issue-bound and rows of 256 columns need 2-row tiles: the
+    // block-synchronous march measured faster there.
+    t.pipe = g.storage == kStoreF32 && t.tpr <= 128;
+    if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v) != 0;  // tuning sweeps
+    if (t.pipe) max_smem = std::max(max_smem, 112 * 1024);  // 4 ring + 3 stage planes: two CTAs per SM
     // rows per tile: at least one round of rows in parallel, 4 by default
     // (measured best on 128x256x128), fewer if shared memory
     // (3*(ty+2) + 2*11*ty) * tpr * 4 bytes does not fit
     int ty = std::max(4, rpt);
     if (const char *v = std::getenv("MCG_FUSED_TY")) ty = std::max(1, std::atoi(v));  // tuning sweeps
-    while (ty > 1 && (3 * (ty + 2) + 2 * kMomCount * ty) * per_row > max_smem) --ty;
+    auto smem_of = [&](int h) {
+        return (t.pipe ? kPipeRing * (h + 2) + kPipeStage * kMomCount * h : 3 * (h + 2) + 2 * kMomCount * h) * per_row;
+    };
+    while (ty > 1 && smem_of(ty) > max_smem) --ty;
     if (ty > rpt) ty -= ty % rpt;  // whole rounds of rows in parallel
     t.ty = ty;
     t.ny_tiles = (g.NY - 2 + ty - 1) / ty;
@@ -1626,10 +1712,20 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     if (chunks < 1) chunks = 1;
     int lz = (g.NZ - 2 + chunks - 1) / chunks;
     if (lz < 4) lz = 4;
+    if (t.pipe) {
+        // 16-plane chunks (measured best: 1.7 waves of two CTAs per SM on
+        // 128x256x128); grids that give fewer than 1.5 waves at that length keep
+        // the block-synchronous march, whose shorter chunks fill the GPU
+        const int ctas16 = t.ny_tiles * ((g.NZ - 2 + 15) / 16);
+        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = 16;
+        else if (!std::getenv("MCG_FUSED_PIPE")) t.pipe = 0;
+    }
     if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
     t.lz = lz;
     t.nz_chunks = (g.NZ - 2 + lz - 1) / lz;
-    t.smem_bytes = (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
+    if (t.cluster > 1) t.pipe = 0;
+    t.smem_bytes = t.pipe ? (kPipeRing * (ty + 2) + kPipeStage * kMomCount * ty) * per_row
+                          : (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
     // bulk prefetch needs 16-byte aligned segments of a multiple of 16 bytes:
     // NX even (float32 rows of 6 NX floats) or a multiple of 4 (float16, 3 NX words)
     t.prefetch = 0;

@@ -84,6 +84,7 @@ struct FusedTiling {
     int smem_bytes;
     int prefetch;  // planes ahead whose source rows are prefetched into L2 (0: off)
     int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
+    int pipe;      // software-pipelined march (k_fused_pipe): one barrier per plane
 };
 
 struct DeviceState {
