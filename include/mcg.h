@@ -283,6 +283,19 @@ mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *r
 mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nsteps, int32_t snapshots,
                            double *J, double *dJ_dsigma, double *dJ_dtau, float *dJ_du0,
                            int64_t *forward_steps, float *ms);
+/* Discrete adjoint of nsteps steps of the jet (MCG_BOUNDARY_JET, float32
+ * storage) from the handle's current state, boundary conditions included: the
+ * inlet (jet/boundary_conditions.cuh:17-85) with its radial profile
+ * (mcg_set_inlet_bessel) and the convective outlet with its carried state
+ * (:163-233).  J = sum over steps t in [t_begin, t_end] of (1/2) sum of uy^2
+ * over interior nodes with y >= y_obs, uy of the fields step t computes (the
+ * velocity of the populations it pulls).  dJ_dc[MCG_INLET_BESSEL_MAX]: the
+ * gradient with respect to the profile coefficients c_k (at the current ones,
+ * for all k including unset ones).  The sweep keeps a tape of every step's
+ * moment record and outlet state (about 48 B per node and step).  The handle's
+ * state is left as it was. */
+mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
+                               double *J, double *dJ_dc, int64_t *forward_steps, float *ms);
 /* The treeverse schedule without running it (host only, no device needed):
  * fused steps a reverse sweep over nsteps steps with `snapshots` held states
  * runs, and the recomputation depth r (least r with C(s + r, s) >= nsteps + 1,

@@ -319,4 +319,147 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
     return MCG_OK;
 }
 
+
+namespace {
+// J0(alpha_k r / R) of every column, k < kInletBesselMax (the inlet profile's basis).
+std::vector<float> bessel_basis(const mcg_params &p) {
+    const int NX = p.NX, NZ = p.NZ, nb = mcg::kInletBesselMax;
+    std::vector<float> b(size_t(nb) * NX * NZ);
+    for (int k = 0; k < nb; ++k) {
+        double a = (double(k + 1) - 0.25) * M_PI;  // k-th zero of J0: Newton from McMahon's estimate
+        for (int it = 0; it < 60; ++it) {
+            const double dx = std::cyl_bessel_j(0.0, a) / -std::cyl_bessel_j(1.0, a);
+            a -= dx;
+            if (std::fabs(dx) < 1e-15 * a) break;
+        }
+        for (int z = 0; z < NZ; ++z)
+            for (int x = 0; x < NX; ++x) {
+                const double dx = double(float(x) - p.jet_x0), dz = double(float(z) - p.jet_z0);
+                const double r = std::sqrt(dx * dx + dz * dz);
+                b[(size_t(k) * NZ + z) * NX + x] = float(std::cyl_bessel_j(0.0, a * r / double(p.jet_radius)));
+            }
+    }
+    return b;
+}
+}  // namespace
+
+mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
+                               double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
+    if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+    if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
+        return fail(MCG_ERR_INVALID_ARG, "need 0 <= t_begin <= t_end < nsteps");
+    if (h->p.boundary != MCG_BOUNDARY_JET || h->p.storage != MCG_STORAGE_F32)
+        return fail(MCG_ERR_UNSUPPORTED, "the jet adjoint covers the jet boundary with float32 storage");
+    if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
+    const mcg::Geometry &g = h->s.g;
+    const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
+    const size_t pop_bytes = size_t(g.slots) * N * sizeof(float);
+    const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
+    const int nb = mcg::kInletBesselMax;
+
+    DeviceBuffers buf;
+    void *p = nullptr;
+    mcg::DeviceState run = h->s;
+    void *work[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint work buffers");
+        work[k] = p;
+    }
+    // both buffers: slots no kernel rewrites carry their initial values in both
+    ADJ_CUDA(cudaMemcpyAsync(work[0], h->s.pops[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream), "copy state");
+    ADJ_CUDA(cudaMemcpyAsync(work[1], h->s.pops[h->cur ^ 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+             "copy state");
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment planes");
+    run.mom = static_cast<float *>(p);
+    ADJ_CUDA(cudaMemcpyAsync(run.mom, h->s.mom, size_t(mcg::kMomCount) * N * sizeof(float), cudaMemcpyDeviceToDevice,
+                             h->stream),
+             "copy moments");
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "jet adjoint psi planes");
+        run.psi[k] = static_cast<float *>(p);
+        ADJ_CUDA(cudaMemcpyAsync(run.psi[k], h->s.psi[k], N * sizeof(float), cudaMemcpyDeviceToDevice, h->stream),
+                 "copy psi");
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
+    run.bmom = static_cast<float *>(p);
+    float *tape = nullptr;
+    ADJ_CUDA(buf.alloc(&p, size_t(nsteps) * rec_floats * sizeof(float)), "jet adjoint moment tape");
+    tape = static_cast<float *>(p);
+    float *lam[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint lambda buffers");
+        lam[k] = static_cast<float *>(p);
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment adjoints");
+    float *lmom = static_cast<float *>(p);
+    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "jet adjoint gradient adjoints");
+    float *lf = static_cast<float *>(p);
+    float *LB[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint outlet adjoints");
+        LB[k] = static_cast<float *>(p);
+    }
+    const std::vector<float> basis = bessel_basis(h->p);
+    ADJ_CUDA(buf.alloc(&p, basis.size() * sizeof(float)), "jet adjoint profile basis");
+    float *dbasis = static_cast<float *>(p);
+    ADJ_CUDA(cudaMemcpyAsync(dbasis, basis.data(), basis.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+             "upload profile basis");
+    ADJ_CUDA(buf.alloc(&p, (2 + size_t(nb)) * sizeof(double)), "jet adjoint accumulators");
+    double *acc = static_cast<double *>(p);  // [0] J, [1] (unused), [2..] dJ/dc_k
+    double *dacc_w = nullptr;
+    ADJ_CUDA(buf.alloc(&p, 2 * sizeof(double)), "jet adjoint parameter partials");
+    dacc_w = static_cast<double *>(p);
+
+    const int64_t step0 = h->step;
+    ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
+    // ---- forward: T steps, each recording its moments, its psi (ghost values
+    // included, as the step reads them) and the outlet state before its boundary
+    for (int64_t t = 0; t < nsteps; ++t) {
+        float *rec = tape + size_t(t) * rec_floats;
+        mcg::DeviceState d = run;
+        d.pops[0] = work[t & 1];
+        d.pops[1] = work[(t + 1) & 1];
+        ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, h->stream),
+                 "record psi");
+        ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
+                   "jet adjoint: record outlet state");
+        d.tape = rec;
+        ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "jet adjoint: forward step");
+        d.tape = nullptr;
+        ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
+        h->launches += 1;
+    }
+    // ---- reverse
+    int lc = 0, lb = 0;
+    for (int64_t t = nsteps - 1; t >= 0; --t) {
+        const float *rec = tape + size_t(t) * rec_floats;
+        const bool in_window = t >= t_begin && t <= t_end;
+        const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
+        ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
+                   "jet adjoint: collision");
+        ADJ_LAUNCH(h,
+                   mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
+                                            lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
+                   "jet adjoint: boundary");
+        ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream), "jet adjoint: moments");
+        lc ^= 1;
+        lb ^= 1;
+    }
+    ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
+    std::vector<double> out(2 + size_t(nb));
+    ADJ_CUDA(cudaMemcpyAsync(out.data(), acc, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+             "download J");
+    ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint run");
+    float t_ms = 0.f;
+    ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
+    if (J) *J = out[0];
+    if (dJ_dc)
+        for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
+    if (forward_steps) *forward_steps = nsteps;
+    if (ms) *ms = t_ms;
+    return MCG_OK;
+}
+
 }  // extern "C"

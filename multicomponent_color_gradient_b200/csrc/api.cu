@@ -443,6 +443,8 @@ double bessel_j0_zero(int k) {
 }
 }  // namespace
 
+static_assert(mcg::kInletBesselMax == MCG_INLET_BESSEL_MAX, "inlet profile size");
+
 mcg_status mcg_set_inlet_bessel(mcg_handle *h, const float *coeffs, int32_t n) {
     if (mcg_status s = check_handle(h)) return s;
     MCG_REQUIRE(n >= 0 && n <= MCG_INLET_BESSEL_MAX, "n must be in [0, MCG_INLET_BESSEL_MAX]");

@@ -576,7 +576,7 @@ __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, 
 #pragma unroll
                 for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
             }
-            if (std::is_same<C, CodecF32>::value && kPeriodic && s.tape) {
+            if (std::is_same<C, CodecF32>::value && s.tape) {
                 // moment record of the pulled state (the adjoint sweep reads it)
                 float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
                 const size_t N = g.N;
@@ -1350,8 +1350,10 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
 // Opposite directions i, i+1 are taken together: feq and fneq split into even
 // and odd parts, Omega2 is even and D odd, so every sum needs only
 // lg_i + lg_o, lg_i - lg_o, ld_i + ld_o and ld_i - ld_o.
+template <bool kPeriodic>
 __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState s, const float *__restrict__ M,
-                                                             const float *lam, float *lmom, float *lf, double *acc) {
+                                                             const float *lam, float *lmom, float *lf, double *acc,
+                                                             AdjObjective obj) {
     __shared__ double sh[kBX * kBY / 32];
     const Geometry &g = s.g;
     const Physics &ph = s.ph;
@@ -1359,7 +1361,7 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
     const bool in = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
-    double a_omega = 0.0, a_Ah = 0.0;
+    double a_omega = 0.0, a_Ah = 0.0, a_J = 0.0;
     if (in) {
         const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
         const size_t N = g.N;
@@ -1377,10 +1379,15 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         float Fx = 0.f, Fy = 0.f, Fz = 0.f, absF = 0.f, K = 0.f;
         bool has_dir = false;
         if (interface) {
+            // periodic box: neighbours wrap over the interior; jet: the record's
+            // psi plane holds the ghost values the forward step read unwrapped
             const float *psi = M + size_t(kTapePsi) * N;
-            const int xn[3] = {wrap_interior(x - 1, g.NX), x, wrap_interior(x + 1, g.NX)};
-            const int yn[3] = {g.sy * wrap_interior(y - 1, g.NY), g.sy * y, g.sy * wrap_interior(y + 1, g.NY)};
-            const int zn[3] = {g.sz * wrap_interior(z - 1, g.NZ), g.sz * z, g.sz * wrap_interior(z + 1, g.NZ)};
+            const int xn[3] = {kPeriodic ? wrap_interior(x - 1, g.NX) : x - 1, x,
+                               kPeriodic ? wrap_interior(x + 1, g.NX) : x + 1};
+            const int yn[3] = {g.sy * (kPeriodic ? wrap_interior(y - 1, g.NY) : y - 1), g.sy * y,
+                               g.sy * (kPeriodic ? wrap_interior(y + 1, g.NY) : y + 1)};
+            const int zn[3] = {g.sz * (kPeriodic ? wrap_interior(z - 1, g.NZ) : z - 1), g.sz * z,
+                               g.sz * (kPeriodic ? wrap_interior(z + 1, g.NZ) : z + 1)};
             float sx = 0.f, sy = 0.f, sz = 0.f;
             static_for<kQ - 1>([&](auto I) {
                 constexpr int i = decltype(I)::value + 1;
@@ -1533,8 +1540,14 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         const float l_rho = l_rhoeq * invr;  // feq is proportional to rho
         lmom[kMomRR * N + id] = l_rho + l_d * rb * inv2 + lK * ph.beta * rb * rb * inv2;
         lmom[kMomRB * N + id] = l_rho - l_d * rr * inv2 + lK * ph.beta * rr * rr * inv2;
+        // the objective's source: J_t = (w/2) sum uy^2 over nodes with y >= y_obs
+        float lobj = 0.f;
+        if (obj.weight != 0.0f && y >= obj.y_obs) {
+            lobj = obj.weight * uy;
+            a_J = 0.5 * double(obj.weight) * double(uy) * double(uy);
+        }
         lmom[kMomUX * N + id] = lux;
-        lmom[kMomUY * N + id] = luy;
+        lmom[kMomUY * N + id] = luy + lobj;
         lmom[kMomUZ * N + id] = luz;
         lmom[kMomPXX * N + id] = lPxx;
         lmom[kMomPXY * N + id] = lPxy;
@@ -1550,15 +1563,18 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
     }
     const double r0 = block_sum_any(a_omega, sh, kBX * kBY);
     const double r1 = block_sum_any(a_Ah, sh, kBX * kBY);
+    const double r2 = obj.J ? block_sum_any(a_J, sh, kBX * kBY) : 0.0;
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicAdd(acc, r0);
         atomicAdd(acc + 1, r1);
+        if (obj.J) atomicAdd(obj.J, r2);
     }
 }
 
 // Per node: the psi-adjoint gathered from the neighbours' F-adjoints, then back
 // through the moments to the 54 pulled populations, stored at their pull
 // sources (transposed streaming) in lam_out.
+template <bool kPeriodic>
 __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *__restrict__ M,
                                                           const float *lmom, const float *lf, float *lam_out) {
     const Geometry &g = s.g;
@@ -1572,13 +1588,20 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const float rho = rr + rb;
-    // psi(y) enters F(y - c_j) with weight w_j c_j / cs2 (periodic neighbours)
+    // psi(y) enters F(y - c_j) with weight w_j c_j / cs2: periodic neighbours
+    // wrap; otherwise only interior neighbours relax (and read psi(y))
     float lpsi = 0.f;
     static_for<kQ - 1>([&](auto I) {
         constexpr int i = decltype(I)::value + 1;
         using D = Dir<i>;
-        const int xn = wrap_interior(x - D::cx, g.NX), yn = wrap_interior(y - D::cy, g.NY),
-                  zn = wrap_interior(z - D::cz, g.NZ);
+        int xn = x - D::cx, yn = y - D::cy, zn = z - D::cz;
+        if constexpr (kPeriodic) {
+            xn = wrap_interior(xn, g.NX);
+            yn = wrap_interior(yn, g.NY);
+            zn = wrap_interior(zn, g.NZ);
+        } else {
+            if (xn < 1 || xn > g.NX - 2 || yn < 1 || yn > g.NY - 2 || zn < 1 || zn > g.NZ - 2) return;
+        }
         const uint32_t nid = uint32_t(xn) + uint32_t(g.sy) * uint32_t(yn) + uint32_t(g.sz) * uint32_t(zn);
         float dot = 0.f;
         if constexpr (D::cx != 0) dot += D::fx * lf[0 * N + nid];
@@ -1601,7 +1624,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     const float invr = 1.0f / rho;
     const float ljx = lux * invr, ljy = luy * invr, ljz = luz * invr;
     lrho -= (lux * ux + luy * uy + luz * uz) * invr;
-    const PullMap<CodecF32> pm(g, x, y, z, true);
+    const PullMap<CodecF32> pm(g, x, y, z, kPeriodic);
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         using D = Dir<i>;
@@ -1619,6 +1642,238 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
         lam_out[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrr + lgi;
         lam_out[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrb + lgi;
     });
+}
+
+// Adjoint of the regularised non-equilibrium part over a set of directions:
+// S2 = sum mu_i H2_i, S3 = sum mu_i H3_i with mu_i = (1-omega) lambda_i w_i give
+// the adjoints of Pi (pxx, pxy, pyy, pyz, pzz, pxz) and the u added through
+// the third-order terms a3 (lbm.cuh:38-78).
+__device__ __forceinline__ void neq_adjoint(const float (&S2)[6], const float (&S3)[7], const NeqTerms &n, float ux,
+                                            float uy, float uz, float (&lP)[6], float (&lu)[3]) {
+    const float c2 = kInv2Cs4, c3 = kInv2Cs6;
+    float lPxx = S2[0] * c2, lPxy = 2.0f * S2[1] * c2, lPyy = S2[2] * c2;
+    float lPyz = 2.0f * S2[3] * c2, lPzz = S2[4] * c2, lPxz = 2.0f * S2[5] * c2;
+    const float la_xxy = S3[0] * c3, la_xxz = S3[1] * c3, la_xyy = S3[2] * c3, la_xzz = S3[3] * c3;
+    const float la_yyz = S3[4] * c3, la_yzz = S3[5] * c3, la_xyz = 2.0f * S3[6] * c3;
+    lPxx += la_xxy * uy + la_xxz * uz;
+    lPyy += la_xyy * ux + la_yyz * uz;
+    lPzz += la_xzz * ux + la_yzz * uy;
+    lPxy += 2.0f * la_xxy * ux + 2.0f * la_xyy * uy + la_xyz * uz;
+    lPxz += 2.0f * la_xxz * ux + 2.0f * la_xzz * uz + la_xyz * uy;
+    lPyz += 2.0f * la_yyz * uy + 2.0f * la_yzz * uz + la_xyz * ux;
+    lu[0] += 2.0f * la_xxy * n.pxy + 2.0f * la_xxz * n.pxz + la_xyy * n.pyy + la_xzz * n.pzz + la_xyz * n.pyz;
+    lu[1] += la_xxy * n.pxx + 2.0f * la_xyy * n.pxy + 2.0f * la_yyz * n.pyz + la_yzz * n.pzz + la_xyz * n.pxz;
+    lu[2] += la_xxz * n.pxx + 2.0f * la_xzz * n.pxz + la_yyz * n.pyy + 2.0f * la_yzz * n.pyz + la_xyz * n.pxy;
+    lP[0] = lPxx; lP[1] = lPxy; lP[2] = lPyy; lP[3] = lPyz; lP[4] = lPzz; lP[5] = lPxz;
+}
+
+template <int I>
+__device__ __forceinline__ void neq_accumulate(float mu, float (&S2)[6], float (&S3)[7]) {
+    using D = Dir<I>;
+    S2[0] += mu * D::Hxx; S2[1] += mu * D::Hxy; S2[2] += mu * D::Hyy;
+    S2[3] += mu * D::Hyz; S2[4] += mu * D::Hzz; S2[5] += mu * D::Hxz;
+    if constexpr (D::Hxxy != 0.0f) S3[0] += mu * D::Hxxy;
+    if constexpr (D::Hxxz != 0.0f) S3[1] += mu * D::Hxxz;
+    if constexpr (D::Hxyy != 0.0f) S3[2] += mu * D::Hxyy;
+    if constexpr (D::Hxzz != 0.0f) S3[3] += mu * D::Hxzz;
+    if constexpr (D::Hyyz != 0.0f) S3[4] += mu * D::Hyyz;
+    if constexpr (D::Hyzz != 0.0f) S3[5] += mu * D::Hyzz;
+    if constexpr (D::Hxyz != 0.0f) S3[6] += mu * D::Hxyz;
+}
+
+__device__ __forceinline__ float inlet_noise_factor(const Physics &ph, int64_t step, int x, int z) {
+    if (ph.inlet_noise == 0.0f) return 1.0f;
+    const float u = hash_uniform(ph.seed, 0x1A1E7ull ^ uint64_t(step), uint64_t(x), uint64_t(z));
+    return 1.0f + (2.0f * u - 1.0f) * ph.inlet_noise;
+}
+
+// One thread per interior column (x, z): the outlet at y = NY-1 and, in a jet
+// column, the inlet at y = 0.  A ghost-plane slot enters only if an interior
+// node pulls it (the boundary also writes slots nothing reads).
+__global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64_t step, const float *__restrict__ M,
+                                                      const float *__restrict__ Bt, const float *__restrict__ lam,
+                                                      const float *__restrict__ lf, float *lmom,
+                                                      const float *__restrict__ LB_in, float *LB_out,
+                                                      const float *__restrict__ bessel, int nb, double *dJdc) {
+    const Geometry &g = s.g;
+    const Physics &ph = s.ph;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool col = x >= 1 && x <= g.NX - 2 && z >= 1 && z <= g.NZ - 2;
+    const size_t N = g.N;
+    const int NP = g.NX * g.NZ;
+    const int ic = x + g.NX * z;
+    float dc[kInletBesselMax];
+#pragma unroll
+    for (int k = 0; k < kInletBesselMax; ++k) dc[k] = 0.f;
+    auto pulled = [&](int xp, int zp) { return xp >= 1 && xp <= g.NX - 2 && zp >= 1 && zp <= g.NZ - 2; };
+    if (col) {
+        // ---------------- outlet (boundary_conditions.cuh:163-233)
+        const uint32_t idF = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 2) + uint32_t(g.sz) * uint32_t(z);
+        const float phi[5] = {M[kMomRR * N + idF], M[kMomRB * N + idF], M[kMomUX * N + idF], M[kMomUY * N + idF],
+                              M[kMomUZ * N + idF]};
+        const NeqTerms nF = make_neq(M[kMomPXX * N + idF], M[kMomPXY * N + idF], M[kMomPYY * N + idF],
+                                     M[kMomPYZ * N + idF], M[kMomPZZ * N + idF], M[kMomPXZ * N + idF], phi[2], phi[3],
+                                     phi[4]);
+        float B[5], Bn[5];
+        const float uc = clamp01(phi[3]);
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            B[c] = Bt[c * NP + ic];
+            Bn[c] = B[c] - uc * (B[c] - phi[c]);
+        }
+        const float rho = Bn[0] + Bn[1];
+        const float inv = 1.0f / rho;
+        const float aR = Bn[0] * inv, aB = Bn[1] * inv;
+        const float oms = 1.0f - omega_at(ph, g.NY - 2);
+        const EqTerms e = make_eq(Bn[2], Bn[3], Bn[4]);
+        float lrho = 0.f, le[3] = {0.f, 0.f, 0.f}, laR = 0.f, laB = 0.f;
+        float S2[6] = {0, 0, 0, 0, 0, 0}, S3[7] = {0, 0, 0, 0, 0, 0, 0};
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            using D = Dir<i>;
+            if constexpr (D::cy == -1) {
+                if (!pulled(x + D::cx, z + D::cz)) return;
+                const float lr = lam[pop_index(g, slot_f32(i, 0), x, g.NY - 1, z)];
+                const float lb = lam[pop_index(g, slot_f32(i, 1), x, g.NY - 1, z)];
+                const float fe = feq<i>(rho, e), fn = fneq<i>(nF);
+                const float gi = fe + oms * fn;
+                const float lg = aR * lr + aB * lb;
+                laR += lr * gi;
+                laB += lb * gi;
+                lrho += lg * fe * inv;
+                float cu = 0.f;
+                if constexpr (D::cx != 0) cu += D::fx * e.ux;
+                cu += D::fy * e.uy;
+                if constexpr (D::cz != 0) cu += D::fz * e.uz;
+                const float P = kInvCs2 + cu * (2.0f * kInv2Cs4) + (cu * cu) * (3.0f * kInv6Cs6) - e.usq * kInv2Cs4;
+                const float Q = kInvCs2 + cu * (2.0f * kInv2Cs4);
+                const float wl = lg * D::w * rho;
+                if constexpr (D::cx != 0) le[0] += wl * P * D::fx;
+                le[1] += wl * P * D::fy;
+                if constexpr (D::cz != 0) le[2] += wl * P * D::fz;
+                const float q = wl * Q;
+                le[0] -= q * e.ux;
+                le[1] -= q * e.uy;
+                le[2] -= q * e.uz;
+                neq_accumulate<i>(oms * lg * D::w, S2, S3);
+            }
+        });
+        const float inv2 = inv * inv;
+        float lBn[5];
+        lBn[0] = lrho + (laR - laB) * Bn[1] * inv2;
+        lBn[1] = lrho - (laR - laB) * Bn[0] * inv2;
+        lBn[2] = le[0];
+        lBn[3] = le[1];
+        lBn[4] = le[2];
+        float luc = 0.f, lphi[5], lB[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            lBn[c] += LB_in[c * NP + ic];
+            luc += lBn[c] * (phi[c] - B[c]);
+            lphi[c] = uc * lBn[c];
+            lB[c] = (1.0f - uc) * lBn[c];
+        }
+        if (phi[3] > 0.0f && phi[3] < 1.0f) lphi[3] += luc;  // d clamp01 / d uy
+        float lP[6], lu[3] = {0.f, 0.f, 0.f};
+        neq_adjoint(S2, S3, nF, phi[2], phi[3], phi[4], lP, lu);
+        lmom[kMomRR * N + idF] += lphi[0];
+        lmom[kMomRB * N + idF] += lphi[1];
+        lmom[kMomUX * N + idF] += lphi[2] + lu[0];
+        lmom[kMomUY * N + idF] += lphi[3] + lu[1];
+        lmom[kMomUZ * N + idF] += lphi[4] + lu[2];
+        lmom[kMomPXX * N + idF] += lP[0];
+        lmom[kMomPXY * N + idF] += lP[1];
+        lmom[kMomPYY * N + idF] += lP[2];
+        lmom[kMomPYZ * N + idF] += lP[3];
+        lmom[kMomPZZ * N + idF] += lP[4];
+        lmom[kMomPXZ * N + idF] += lP[5];
+        // psi(B) at (x, NY-1, z) entered the colour gradient of the step's
+        // interior nodes (x, NY-2, z) - c over the cy = +1 directions
+        float lpsi = 0.f;
+        static_for<kQ>([&](auto I) {
+            constexpr int i = decltype(I)::value;
+            using D = Dir<i>;
+            if constexpr (D::cy == 1) {
+                const int xn = x - D::cx, zn = z - D::cz;
+                if (!pulled(xn, zn)) return;
+                const uint32_t nid = uint32_t(xn) + uint32_t(g.sy) * uint32_t(g.NY - 2) + uint32_t(g.sz) * uint32_t(zn);
+                float dot = D::fy * lf[1 * N + nid];
+                if constexpr (D::cx != 0) dot += D::fx * lf[0 * N + nid];
+                if constexpr (D::cz != 0) dot += D::fz * lf[2 * N + nid];
+                lpsi += D::w * dot;
+            }
+        });
+        lpsi *= kInvCs2;
+        const float rB = B[0] + B[1];
+        const float i2 = 1.0f / (rB * rB);
+        lB[0] += lpsi * 2.0f * B[1] * i2;
+        lB[1] -= lpsi * 2.0f * B[0] * i2;
+#pragma unroll
+        for (int c = 0; c < 5; ++c) LB_out[c * NP + ic] = lB[c];
+        // ---------------- inlet (boundary_conditions.cuh:17-85): jet columns only
+        if (is_jet_column(ph, x, z)) {
+            const uint32_t id1 = uint32_t(x) + uint32_t(g.sy) * 1u + uint32_t(g.sz) * uint32_t(z);
+            const float u1x = M[kMomUX * N + id1], u1y = M[kMomUY * N + id1], u1z = M[kMomUZ * N + id1];
+            const NeqTerms n1 = make_neq(M[kMomPXX * N + id1], M[kMomPXY * N + id1], M[kMomPYY * N + id1],
+                                         M[kMomPYZ * N + id1], M[kMomPZZ * N + id1], M[kMomPXZ * N + id1], u1x, u1y,
+                                         u1z);
+            const float rT = ph.rhob0;  // the mask: red 0, blue rhob0 (aR = 0, aB = 1)
+            const float U = inlet_velocity(s, step, x, z);
+            const float omsb = 1.0f - ph.omega_b;
+            float lU = 0.f;
+            float T2[6] = {0, 0, 0, 0, 0, 0}, T3[7] = {0, 0, 0, 0, 0, 0, 0};
+            static_for<kQ>([&](auto I) {
+                constexpr int i = decltype(I)::value;
+                using D = Dir<i>;
+                if constexpr (D::cy == 1) {
+                    if (!pulled(x + D::cx, z + D::cz)) return;
+                    const float lg = lam[pop_index(g, slot_f32(i, 1), x, 0, z)];  // red = 0 * g
+                    // d feq_i / d uy at u = (0, U, 0): w rho (c_y P - U Q), c.u = U
+                    const float P = kInvCs2 + U * (2.0f * kInv2Cs4) + (U * U) * (3.0f * kInv6Cs6) - (U * U) * kInv2Cs4;
+                    const float Q = kInvCs2 + U * (2.0f * kInv2Cs4);
+                    lU += lg * D::w * rT * (P - U * Q);
+                    neq_accumulate<i>(omsb * lg * D::w, T2, T3);
+                }
+            });
+            float lP1[6], lu1[3] = {0.f, 0.f, 0.f};
+            neq_adjoint(T2, T3, n1, u1x, u1y, u1z, lP1, lu1);
+            lmom[kMomUX * N + id1] += lu1[0];
+            lmom[kMomUY * N + id1] += lu1[1];
+            lmom[kMomUZ * N + id1] += lu1[2];
+            lmom[kMomPXX * N + id1] += lP1[0];
+            lmom[kMomPXY * N + id1] += lP1[1];
+            lmom[kMomPYY * N + id1] += lP1[2];
+            lmom[kMomPYZ * N + id1] += lP1[3];
+            lmom[kMomPZZ * N + id1] += lP1[4];
+            lmom[kMomPXZ * N + id1] += lP1[5];
+            // U = U0 (1 + sum_k c_k J0_k) (1 + noise): dU/dc_k = U0 (1 + noise) J0_k
+            if (bessel) {
+                const float dU = ph.jet_velocity * inlet_noise_factor(ph, step, x, z);
+                for (int k = 0; k < nb; ++k) dc[k] = lU * dU * bessel[k * NP + ic];
+            }
+        }
+    }
+    if (bessel) {
+        for (int k = 0; k < nb; ++k) {
+            double v = dc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFull, v, o);
+            if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(dJdc + k, v);
+        }
+    }
+}
+
+// Outlet state (rr, rb, ux, uy, uz at y = NY-1) of interior columns to dst[5][NX*NZ].
+__global__ void __launch_bounds__(256) k_copy_outlet_state(const DeviceState s, float *dst) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.NX || z >= g.NZ) return;
+    const uint32_t idB = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 1) + uint32_t(g.sz) * uint32_t(z);
+    const int NP = g.NX * g.NZ;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) dst[c * NP + x + g.NX * z] = s.mom[size_t(c) * g.N + idB];
 }
 
 // dJ/du0 for an initial state f0_c,i = feq_i(rho_c, u0): pulls lambda_0 like
@@ -1852,12 +2107,42 @@ cudaError_t launch_adj_terminal(const DeviceState &s, const float *M, const floa
     return cudaGetLastError();
 }
 
+cudaError_t launch_adj_collide(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
+                               double *acc, const AdjObjective &obj, cudaStream_t st) {
+    if (s.g.boundary == kBoundaryPeriodic)
+        k_adj_collide<true><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lam_in, lmom, lf, acc, obj);
+    else
+        k_adj_collide<false><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lam_in, lmom, lf, acc, obj);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adj_moments(const DeviceState &s, const float *M, const float *lmom, const float *lf,
+                               float *lam_out, cudaStream_t st) {
+    if (s.g.boundary == kBoundaryPeriodic)
+        k_adj_moments<true><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lmom, lf, lam_out);
+    else
+        k_adj_moments<false><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lmom, lf, lam_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_adj_step(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
                             float *lam_out, double *acc, cudaStream_t st) {
-    k_adj_collide<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lam_in, lmom, lf, acc);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_adj_collide(s, M, lam_in, lmom, lf, acc, AdjObjective{0.0f, 0, nullptr}, st);
     if (e != cudaSuccess) return e;
-    k_adj_moments<<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, M, lmom, lf, lam_out);
+    return launch_adj_moments(s, M, lmom, lf, lam_out, st);
+}
+
+cudaError_t launch_adj_boundary(const DeviceState &s, int64_t step, const float *M, const float *Bt,
+                                const float *lam_next, const float *lf, float *lmom, const float *LB_in,
+                                float *LB_out, const float *bessel, int nb, double *dJdc, cudaStream_t st) {
+    const dim3 block(32, 8), grid((s.g.NX + 31) / 32, (s.g.NZ + 7) / 8);
+    k_adj_boundary<<<grid, block, 0, st>>>(s, step, M, Bt, lam_next, lf, lmom, LB_in, LB_out, bessel, nb, dJdc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_copy_outlet_state(const DeviceState &s, float *dst, cudaStream_t st) {
+    const dim3 block(32, 8), grid((s.g.NX + 31) / 32, (s.g.NZ + 7) / 8);
+    k_copy_outlet_state<<<grid, block, 0, st>>>(s, dst);
     return cudaGetLastError();
 }
 

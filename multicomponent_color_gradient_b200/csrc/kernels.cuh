@@ -32,6 +32,7 @@
 namespace mcg {
 
 enum : int { kBoundaryJet = 0, kBoundaryClosed = 1, kBoundaryPeriodic = 2 };
+constexpr int kInletBesselMax = 8;  // coefficients of the radial inlet profile
 enum : int { kStoreF32 = 0, kStoreF16 = 1 };
 enum : int { kMomRR = 0, kMomRB, kMomUX, kMomUY, kMomUZ, kMomPXX, kMomPXY, kMomPYY, kMomPYZ, kMomPZZ, kMomPXZ, kMomCount };
 // A moment record of one state: the kMomCount moment planes, then psi.
@@ -141,7 +142,15 @@ uint32_t conservation_blocks(const Geometry &g);
 cudaError_t launch_conservation(const DeviceState &s, int cur, double *partials, double *out5, cudaStream_t st);
 cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaStream_t st);
 
-// ---- discrete adjoint of the step (periodic box, float32 populations) ----
+// Objective source of an adjoint step: J_t = (weight/2) sum of uy^2 over
+// interior nodes with y >= y_obs (weight 0: none); J accumulates J_t (or null).
+struct AdjObjective {
+    float weight;
+    int y_obs;
+    double *J;
+};
+
+// ---- discrete adjoint of the step (float32 populations) ----
 // lambda buffers share the population layout; M is the moment record
 // [kTapePlanes][N] of the state the pass belongs to (interior nodes).
 // Terminal condition for J = sum (psi_T - target)^2, one adjoint step
@@ -151,6 +160,26 @@ cudaError_t launch_adj_terminal(const DeviceState &s, const float *M, const floa
                                 cudaStream_t st);
 cudaError_t launch_adj_step(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
                             float *lam_out, double *acc, cudaStream_t st);
+// The same step in two parts for the jet, with the boundary adjoint between
+// them: the relaxation part (lam_in -> lmom, lf, objective source) and the
+// moment part (lmom, lf -> lam_out).
+cudaError_t launch_adj_collide(const DeviceState &s, const float *M, const float *lam_in, float *lmom, float *lf,
+                               double *acc, const AdjObjective &obj, cudaStream_t st);
+cudaError_t launch_adj_moments(const DeviceState &s, const float *M, const float *lmom, const float *lf,
+                               float *lam_out, cudaStream_t st);
+// Adjoint of the jet boundary of step `step` (inlet and convective outlet,
+// jet/boundary_conditions.cuh:17-85,163-233) and of the outlet-plane psi the
+// step read.  M: the step's moment record; Bt: [5][NX*NZ] outlet state
+// (rr, rb, ux, uy, uz at y = NY-1) before the step's boundary; lam_next: the
+// adjoint of the populations the step wrote; lf: the step's colour-gradient
+// adjoint.  Adds into lmom at y = 1 and y = NY-2; LB_in: the adjoint of the
+// outlet state after the boundary, LB_out: before it; bessel: [nb][NX*NZ] J0
+// basis of the inlet profile (or null), dJdc[nb] += dJ/dc_k.
+cudaError_t launch_adj_boundary(const DeviceState &s, int64_t step, const float *M, const float *Bt,
+                                const float *lam_next, const float *lf, float *lmom, const float *LB_in,
+                                float *LB_out, const float *bessel, int nb, double *dJdc, cudaStream_t st);
+// The outlet state (5 planes at y = NY-1, interior columns) to dst[5][NX*NZ].
+cudaError_t launch_copy_outlet_state(const DeviceState &s, float *dst, cudaStream_t st);
 cudaError_t launch_adj_initial(const DeviceState &s, const float *M, const float *lam0, float *du0, cudaStream_t st);
 
 }  // namespace mcg
