@@ -291,11 +291,14 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
  * over interior nodes with y >= y_obs, uy of the fields step t computes (the
  * velocity of the populations it pulls).  dJ_dc[MCG_INLET_BESSEL_MAX]: the
  * gradient with respect to the profile coefficients c_k (at the current ones,
- * for all k including unset ones).  The sweep keeps a tape of every step's
- * moment record and outlet state (about 48 B per node and step).  The handle's
- * state is left as it was. */
+ * for all k including unset ones).  Memory: with segment <= 0 or >= nsteps the
+ * sweep keeps a tape of every step's moment record and outlet state (about
+ * 48 B per node and step) and runs nsteps forward steps; with 0 < segment <
+ * nsteps it keeps a snapshot (populations and outlet state, 216 B per node)
+ * every `segment` steps and the tape of one segment, and runs about
+ * 2*nsteps forward steps.  The handle's state is left as it was. */
 mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
-                               double *J, double *dJ_dc, int64_t *forward_steps, float *ms);
+                               int32_t segment, double *J, double *dJ_dc, int64_t *forward_steps, float *ms);
 /* The treeverse schedule without running it (host only, no device needed):
  * fused steps a reverse sweep over nsteps steps with `snapshots` held states
  * runs, and the recomputation depth r (least r with C(s + r, s) >= nsteps + 1,

@@ -94,7 +94,8 @@ SIGNATURES = {
     "mcg_get_inlet_profile": [_P, _F],
     "mcg_adjoint_run": [_P, _F, C.c_int32, C.c_int32, _D, _D, _D, _F, C.POINTER(C.c_int64), _F],
     "mcg_adjoint_plan": [C.c_int32, C.c_int32, C.POINTER(C.c_int64), _I32],
-    "mcg_adjoint_jet_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.POINTER(C.c_int64), _F],
+    "mcg_adjoint_jet_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.POINTER(C.c_int64),
+                            _F],
     "mcg_output_open": [_P, C.c_char_p],
     "mcg_output_step": [_P, C.c_int32],
     "mcg_write_radial_outputs": [_P],

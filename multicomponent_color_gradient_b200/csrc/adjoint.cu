@@ -344,7 +344,7 @@ std::vector<float> bessel_basis(const mcg_params &p) {
 }  // namespace
 
 mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
-                               double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
+                               int32_t segment, double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
     if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
     if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
     if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
@@ -383,8 +383,20 @@ mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, i
     }
     ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
     run.bmom = static_cast<float *>(p);
+    // segments of L steps: a snapshot (populations + outlet state) at the
+    // start of each, and a tape of one segment's records
+    const int64_t L = (segment <= 0 || segment >= nsteps) ? nsteps : segment;
+    const int64_t nseg = (nsteps + L - 1) / L;
+    std::vector<void *> snap(size_t(nseg), nullptr);
+    std::vector<float *> snapB(size_t(nseg), nullptr);
+    for (int64_t j = 0; j < nseg; ++j) {
+        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint snapshots");
+        snap[size_t(j)] = p;
+        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
+        snapB[size_t(j)] = static_cast<float *>(p);
+    }
     float *tape = nullptr;
-    ADJ_CUDA(buf.alloc(&p, size_t(nsteps) * rec_floats * sizeof(float)), "jet adjoint moment tape");
+    ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
     tape = static_cast<float *>(p);
     float *lam[2];
     for (int k = 0; k < 2; ++k) {
@@ -413,39 +425,67 @@ mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, i
 
     const int64_t step0 = h->step;
     ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
-    // ---- forward: T steps, each recording its moments, its psi (ghost values
-    // included, as the step reads them) and the outlet state before its boundary
-    for (int64_t t = 0; t < nsteps; ++t) {
-        float *rec = tape + size_t(t) * rec_floats;
+    int64_t fwd = 0;
+    // one forward step t of the run's state (work[t & 1] -> work[(t+1) & 1]),
+    // recording into `rec` when given: its psi with the ghost values it reads,
+    // the outlet state before its boundary, and (k_fused) its moments
+    auto forward = [&](int64_t t, float *rec) -> mcg_status {
         mcg::DeviceState d = run;
         d.pops[0] = work[t & 1];
         d.pops[1] = work[(t + 1) & 1];
-        ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
-                                 cudaMemcpyDeviceToDevice, h->stream),
-                 "record psi");
-        ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
-                   "jet adjoint: record outlet state");
-        d.tape = rec;
+        if (rec) {
+            ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, h->stream),
+                     "record psi");
+            ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
+                       "jet adjoint: record outlet state");
+            d.tape = rec;
+        }
         ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "jet adjoint: forward step");
         d.tape = nullptr;
         ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
-        h->launches += 1;
-    }
-    // ---- reverse
+        ++fwd;
+        return MCG_OK;
+    };
+    auto save = [&](int64_t j, int64_t t) -> mcg_status {
+        ADJ_CUDA(cudaMemcpyAsync(snap[size_t(j)], work[t & 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                 "save snapshot");
+        ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(run, snapB[size_t(j)], h->stream), "jet adjoint: save outlet");
+        return MCG_OK;
+    };
+    // ---- pass 1 (several segments only): snapshots at every segment start
+    if (mcg_status st = save(0, 0)) return st;
+    if (nseg > 1)
+        for (int64_t t = 0; t < (nseg - 1) * L; ++t) {
+            if (mcg_status st = forward(t, nullptr)) return st;
+            if ((t + 1) % L == 0)
+                if (mcg_status st = save((t + 1) / L, t + 1)) return st;
+        }
+    // ---- pass 2: per segment from the last, restore, re-run recording, reverse
     int lc = 0, lb = 0;
-    for (int64_t t = nsteps - 1; t >= 0; --t) {
-        const float *rec = tape + size_t(t) * rec_floats;
-        const bool in_window = t >= t_begin && t <= t_end;
-        const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
-        ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
-                   "jet adjoint: collision");
-        ADJ_LAUNCH(h,
-                   mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
-                                            lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
-                   "jet adjoint: boundary");
-        ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream), "jet adjoint: moments");
-        lc ^= 1;
-        lb ^= 1;
+    for (int64_t j = nseg - 1; j >= 0; --j) {
+        const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
+        ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                 "restore snapshot");
+        ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
+                   "jet adjoint: restore outlet");
+        for (int64_t t = s0; t < s1; ++t)
+            if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats)) return st;
+        for (int64_t t = s1 - 1; t >= s0; --t) {
+            const float *rec = tape + size_t(t - s0) * rec_floats;
+            const bool in_window = t >= t_begin && t <= t_end;
+            const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
+            ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
+                       "jet adjoint: collision");
+            ADJ_LAUNCH(h,
+                       mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
+                                                lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
+                       "jet adjoint: boundary");
+            ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream),
+                       "jet adjoint: moments");
+            lc ^= 1;
+            lb ^= 1;
+        }
     }
     ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
     std::vector<double> out(2 + size_t(nb));
@@ -457,7 +497,7 @@ mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, i
     if (J) *J = out[0];
     if (dJ_dc)
         for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
-    if (forward_steps) *forward_steps = nsteps;
+    if (forward_steps) *forward_steps = fwd;
     if (ms) *ms = t_ms;
     return MCG_OK;
 }

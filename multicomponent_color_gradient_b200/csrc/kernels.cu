@@ -1864,6 +1864,21 @@ __global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64
     }
 }
 
+// The inverse: outlet state from src[5][NX*NZ] back to y = NY-1, with the psi
+// the next step reads there (what the boundary launch writes).
+__global__ void __launch_bounds__(256) k_restore_outlet_state(const DeviceState s, const float *src, float *psi) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.NX || z >= g.NZ) return;
+    const uint32_t idB = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 1) + uint32_t(g.sz) * uint32_t(z);
+    const int NP = g.NX * g.NZ;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) s.mom[size_t(c) * g.N + idB] = src[c * NP + x + g.NX * z];
+    if (x >= 1 && x <= g.NX - 2 && z >= 1 && z <= g.NZ - 2)
+        psi[idB] = psi_of(src[0 * NP + x + g.NX * z], src[1 * NP + x + g.NX * z]);
+}
+
 // Outlet state (rr, rb, ux, uy, uz at y = NY-1) of interior columns to dst[5][NX*NZ].
 __global__ void __launch_bounds__(256) k_copy_outlet_state(const DeviceState s, float *dst) {
     const Geometry &g = s.g;
@@ -2137,6 +2152,12 @@ cudaError_t launch_adj_boundary(const DeviceState &s, int64_t step, const float 
                                 float *LB_out, const float *bessel, int nb, double *dJdc, cudaStream_t st) {
     const dim3 block(32, 8), grid((s.g.NX + 31) / 32, (s.g.NZ + 7) / 8);
     k_adj_boundary<<<grid, block, 0, st>>>(s, step, M, Bt, lam_next, lf, lmom, LB_in, LB_out, bessel, nb, dJdc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_restore_outlet_state(const DeviceState &s, const float *src, float *psi, cudaStream_t st) {
+    const dim3 block(32, 8), grid((s.g.NX + 31) / 32, (s.g.NZ + 7) / 8);
+    k_restore_outlet_state<<<grid, block, 0, st>>>(s, src, psi);
     return cudaGetLastError();
 }
 

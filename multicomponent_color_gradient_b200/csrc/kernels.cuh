@@ -178,8 +178,10 @@ cudaError_t launch_adj_moments(const DeviceState &s, const float *M, const float
 cudaError_t launch_adj_boundary(const DeviceState &s, int64_t step, const float *M, const float *Bt,
                                 const float *lam_next, const float *lf, float *lmom, const float *LB_in,
                                 float *LB_out, const float *bessel, int nb, double *dJdc, cudaStream_t st);
-// The outlet state (5 planes at y = NY-1, interior columns) to dst[5][NX*NZ].
+// The outlet state (5 planes at y = NY-1, interior columns) to dst[5][NX*NZ],
+// and back (restoring also the outlet-plane psi in `psi`).
 cudaError_t launch_copy_outlet_state(const DeviceState &s, float *dst, cudaStream_t st);
+cudaError_t launch_restore_outlet_state(const DeviceState &s, const float *src, float *psi, cudaStream_t st);
 cudaError_t launch_adj_initial(const DeviceState &s, const float *M, const float *lam0, float *du0, cudaStream_t st);
 
 }  // namespace mcg

@@ -114,15 +114,16 @@ class Solver:
         assert all(a.size == self.N for a in arrs)
         self._c("mcg_init_equilibrium", *[_fptr(a) for a in arrs])
 
-    def adjoint_jet_run(self, nsteps: int, t_begin: int, t_end: int, y_obs: int) -> Dict:
+    def adjoint_jet_run(self, nsteps: int, t_begin: int, t_end: int, y_obs: int, segment: int = 0) -> Dict:
         """J = sum over steps t_begin..t_end of (1/2) sum_{y >= y_obs} uy^2 and
         dJ/dc of the inlet-profile coefficients (8 values), from one forward +
-        reverse sweep of the jet; the state is unchanged."""
+        reverse sweep of the jet (snapshots every `segment` steps when 0 <
+        segment < nsteps); the state is unchanged."""
         J = C.c_double()
         dc = (C.c_double * 8)()
         fwd, ms = C.c_int64(), C.c_float()
-        self._c("mcg_adjoint_jet_run", int(nsteps), int(t_begin), int(t_end), int(y_obs), C.byref(J), dc,
-                C.byref(fwd), C.byref(ms))
+        self._c("mcg_adjoint_jet_run", int(nsteps), int(t_begin), int(t_end), int(y_obs), int(segment), C.byref(J),
+                dc, C.byref(fwd), C.byref(ms))
         return {"J": J.value, "dJ_dc": np.array(dc[:], np.float64), "forward_steps": int(fwd.value),
                 "ms": float(ms.value)}
 

@@ -82,6 +82,18 @@ def test_dJ_dc_matches_fp64_central_differences(adjoint, k):
     assert abs(g - fd) <= 0.03 * abs(fd), (k, g, fd)
 
 
+@pytest.mark.parametrize("segment", [7, 16])
+def test_segments_give_the_same_gradients(adjoint, segment):
+    with Solver(CASE) as S:
+        S.set_inlet_bessel(C0.astype(np.float32))
+        S.init_jet()
+        r = S.adjoint_jet_run(T, T0, T1, YOBS, segment=segment)
+    nseg = -(-T // segment)
+    assert r["forward_steps"] == (nseg - 1) * segment + T
+    assert abs(r["J"] - adjoint["J"]) <= 1e-12 * adjoint["J"]
+    np.testing.assert_allclose(r["dJ_dc"], adjoint["dJ_dc"], rtol=1e-9, atol=1e-15)
+
+
 def test_state_is_left_unchanged():
     with Solver(CASE) as S:
         S.set_inlet_bessel(C0.astype(np.float32))
