@@ -206,6 +206,27 @@ def adjoint_cost(steps: int):
         P.close()
 
 
+def jet_adjoint_cost(steps: int, segment: int):
+    """Jet adjoint cost on the bench jet (128x256x128): one forward + reverse
+    sweep over `steps` steps (objective over the second half, y >= 64, inlet
+    profile gradient) against `steps` plain forward steps."""
+    import numpy as np
+
+    from multicomponent_color_gradient_b200 import Solver, get_case
+
+    with Solver(get_case(DEFAULT_CASE, NSTATS_START_STEP=10 ** 9)) as S:
+        S.set_inlet_bessel(np.zeros(8, np.float32))
+        S.init_jet()
+        S.adjoint_jet_run(20, 10, 19, 64)  # warm-up
+        r = S.adjoint_jet_run(steps, steps // 2, steps - 1, 64, segment=segment)
+        S.init_jet()
+        S.step(3)
+        fwd = S.step_timed(steps)
+    return {"value": round(r["ms"] / fwd, 3), "unit": "adjoint sweep / forward run", "workload": DEFAULT_CASE,
+            "steps": steps, "segment": segment, "sweep_ms": round(r["ms"], 3), "forward_ms": round(fwd, 3),
+            "forward_steps_in_sweep": r["forward_steps"], "gradient": "inlet-profile Bessel coefficients"}
+
+
 def run_reference(args, world, rank):
     if world > 1 and rank != 0:
         return
@@ -352,12 +373,16 @@ def main():
                "step_frac_216B": round(216 * cells / (ms16 / args.steps * 1e-3) / 1e9 / hbm_peak, 4)}
         S16.close()
 
-    adjoint = None
+    adjoint = jet_adjoint = None
     if not args.no_adjoint:
         try:
             adjoint = adjoint_cost(args.adjoint_steps)
         except Exception as exc:
             adjoint = {"value": None, "error": str(exc)[:200]}
+        try:
+            jet_adjoint = jet_adjoint_cost(400, 100)
+        except Exception as exc:
+            jet_adjoint = {"value": None, "error": str(exc)[:200]}
 
     if rank != 0:
         return
@@ -377,7 +402,7 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (step_bytes / 2 * cells / 1e6)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-        "f16_store": f16, "adjoint": adjoint,
+        "f16_store": f16, "adjoint": adjoint, "jet_adjoint": jet_adjoint,
     }
     print(json.dumps(line))
 
