@@ -529,6 +529,237 @@ struct Oracle {
             ++step;
         }
     }
+
+    // ---------------------------------------------------------------- adjoint
+    // Discrete adjoint of `nsteps` steps of the periodic box in this class's own
+    // form (push into one buffer): for J = sum over interior nodes of
+    // (psi_T - target)^2 with psi_T the colour field of f(T), returns J,
+    // dJ/dsigma, dJ/dtau and dJ/du0 of an initial state f0 = feq(rho_c, u0).
+    // Step t maps f_t -> f_{t+1} by f_{t+1,i}(x + c_i) = C_i(M_t(x), F_t(x)); the
+    // reverse step takes lambda of the pushed values, the collision's Jacobian
+    // at each node (M and F), the gradient stencil's transpose and the moments'
+    // transpose.  The state is left at f(0).
+    void adjoint_periodic(const double *target, int nsteps, double out[3], double *du0) {
+        const size_t NQ = size_t(Q) * N;
+        std::vector<std::vector<T>> hr(size_t(nsteps) + 1), hb(size_t(nsteps) + 1);
+        hr[0] = fr;
+        hb[0] = fb;
+        const int64_t step0 = step;
+        for (int t = 0; t < nsteps; ++t) {
+            run(1);
+            hr[size_t(t) + 1] = fr;
+            hb[size_t(t) + 1] = fb;
+        }
+        std::vector<double> lr(NQ, 0.0), lb(NQ, 0.0), nr(NQ, 0.0), nb(NQ, 0.0);
+        std::vector<double> lm(size_t(11) * N, 0.0), lF(size_t(3) * N, 0.0);
+        double Jv = 0, a_omega = 0, a_Ah = 0;
+        auto load = [&](int t) {
+            fr = hr[size_t(t)];
+            fb = hb[size_t(t)];
+            macros();  // moments of f(t); ghost densities mirrored
+        };
+        // terminal: lambda of f(T) from J
+        load(nsteps);
+        for (int z = 1; z <= NZ - 2; ++z)
+            for (int y = 1; y <= NY - 2; ++y)
+                for (int x = 1; x <= NX - 2; ++x) {
+                    const size_t id = idx(x, y, z);
+                    const double rr = double(rhor[id]), rb = double(rhob[id]), rho = rr + rb;
+                    const double d = (rr - rb) / rho - target[id];
+                    Jv += d * d;
+                    const double lrr = 2 * d * 2 * rb / (rho * rho), lrb = -2 * d * 2 * rr / (rho * rho);
+                    for (int i = 0; i < Q; ++i) {
+                        lr[fidx(id, i)] = lrr;
+                        lb[fidx(id, i)] = lrb;
+                    }
+                }
+        const double A = double(sigma_over_4cs4 / taub), Ah = A / 2;
+        for (int t = nsteps - 1; t >= 0; --t) {
+            load(t);
+            std::fill(lF.begin(), lF.end(), 0.0);
+            // collision adjoint at every interior node
+            for (int z = 1; z <= NZ - 2; ++z)
+                for (int y = 1; y <= NY - 2; ++y)
+                    for (int x = 1; x <= NX - 2; ++x) {
+                        const size_t id = idx(x, y, z);
+                        const double rr = rhor[id], rb = rhob[id], rho = rr + rb;
+                        const double vx = ux[id], vy = uy[id], vz = uz[id];
+                        const double pxx = Pixx[id], pxy = Pixy[id], pyy = Piyy[id], pyz = Piyz[id],
+                                     pzz = Pizz[id], pxz = Pixz[id];
+                        const double usq = vx * vx + vy * vy + vz * vz;
+                        const double aR = rr / rho, aB = rb / rho;
+                        const double oms = 1.0 - double(omega_sponge(y));
+                        const bool iface = !(4.0 * rr * rb / (rho * rho) <= 1e-4);
+                        double Fx = 0, Fy = 0, Fz = 0, absF = 0;
+                        if (iface) {
+                            T fx, fy, fz;
+                            colour_gradient(id, fx, fy, fz);
+                            Fx = fx; Fy = fy; Fz = fz;
+                            absF = std::sqrt(Fx * Fx + Fy * Fy + Fz * Fz);
+                        }
+                        const bool hd = iface && !(absF <= 1e-4);
+                        const double K = beta * rr * rb / rho;
+                        // third-order terms of fneq (lbm.cuh:67-73)
+                        const double a3[7] = {pxx * vy + 2 * pxy * vx, pxx * vz + 2 * pxz * vx, pyy * vx + 2 * pxy * vy,
+                                              pzz * vx + 2 * pxz * vz, pyy * vz + 2 * pyz * vy, pzz * vy + 2 * pyz * vz,
+                                              pxy * vz + pxz * vy + pyz * vx};
+                        double l_aR = 0, l_aB = 0, l_rhoeq = 0, luP[3] = {0, 0, 0}, luQ = 0, l_oms = 0;
+                        double S2[6] = {0, 0, 0, 0, 0, 0}, S3[7] = {0, 0, 0, 0, 0, 0, 0};
+                        double sA[3] = {0, 0, 0}, sB = 0, sD[3] = {0, 0, 0}, sE = 0, sBB = 0, l_Ah = 0;
+                        for (int i = 0; i < Q; ++i) {
+                            const double cx = CX[i], cy = CY[i], cz = CZ[i];
+                            const size_t tgt = fidx(idx(wrapx(x + CX[i]), wrapy(y + CY[i]), wrapz(z + CZ[i])), i);
+                            const double Lr = lr[tgt], Lb = lb[tgt];
+                            const double w = L.w[i];
+                            const double cu = cx * vx + cy * vy + cz * vz;
+                            const double fe = w * rho *
+                                              (1 + cu * cu / (2 * double(L.cs4)) - usq / (2 * double(L.cs2)) +
+                                               cu / double(L.cs2) + cu * (cu * cu / (6 * double(L.cs6)) - usq / (2 * double(L.cs4))));
+                            const double H2[6] = {L.Hxx[i], L.Hxy[i], L.Hyy[i], L.Hyz[i], L.Hzz[i], L.Hxz[i]};
+                            const double H3[7] = {L.Hxxy[i], L.Hxxz[i], L.Hxyy[i], L.Hxzz[i], L.Hyyz[i], L.Hyzz[i], L.Hxyz[i]};
+                            const double A2 = (pxx * H2[0] + 2 * pxy * H2[1] + pyy * H2[2] + 2 * pyz * H2[3] + pzz * H2[4] +
+                                               2 * pxz * H2[5]) / (2 * double(L.cs4));
+                            double A3 = 0;
+                            for (int k = 0; k < 6; ++k) A3 += a3[k] * H3[k];
+                            A3 += 2 * a3[6] * H3[6];
+                            const double fn = w * (A2 + A3 / (2 * double(L.cs6)));
+                            const double fc = Fx * cx + Fy * cy + Fz * cz;
+                            double om2A = 0;  // Omega2 / (A/2)
+                            if (iface) om2A = absF * (w * ((i != 0 && hd) ? fc * fc / (absF * absF) : 0.0) - double(L.B[i]));
+                            const double gi = fe + oms * fn + Ah * om2A;
+                            l_aR += Lr * gi;
+                            l_aB += Lb * gi;
+                            const double lg = aR * Lr + aB * Lb, ld = Lr - Lb;
+                            l_rhoeq += lg * fe;
+                            const double P = 1 / double(L.cs2) + cu / double(L.cs4) + cu * cu / (2 * double(L.cs6)) -
+                                             usq / (2 * double(L.cs4));
+                            const double Qd = 1 / double(L.cs2) + cu / double(L.cs4);
+                            const double wl = lg * w * rho;
+                            luP[0] += wl * P * cx;
+                            luP[1] += wl * P * cy;
+                            luP[2] += wl * P * cz;
+                            luQ += wl * Qd;
+                            l_oms += lg * fn;
+                            const double mu = oms * lg * w;
+                            for (int k = 0; k < 6; ++k) S2[k] += mu * H2[k];
+                            for (int k = 0; k < 7; ++k) S3[k] += mu * H3[k];
+                            if (iface) {
+                                sBB += lg * double(L.B[i]);
+                                l_Ah += lg * om2A;
+                                if (i != 0 && hd) {
+                                    const double a = lg * w * fc, dd = ld * w * double(L.invc[i]);
+                                    sA[0] += a * cx; sA[1] += a * cy; sA[2] += a * cz;
+                                    sD[0] += dd * cx; sD[1] += dd * cy; sD[2] += dd * cz;
+                                    sB += a * fc;
+                                    sE += dd * fc;
+                                }
+                            }
+                        }
+                        const double c2 = 1 / (2 * double(L.cs4)), c3 = 1 / (2 * double(L.cs6));
+                        double lP[6] = {S2[0] * c2, 2 * S2[1] * c2, S2[2] * c2, 2 * S2[3] * c2, S2[4] * c2, 2 * S2[5] * c2};
+                        const double la[7] = {S3[0] * c3, S3[1] * c3, S3[2] * c3, S3[3] * c3, S3[4] * c3, S3[5] * c3,
+                                              2 * S3[6] * c3};
+                        // a3: xxy, xxz, xyy, xzz, yyz, yzz, xyz
+                        lP[0] += la[0] * vy + la[1] * vz;
+                        lP[2] += la[2] * vx + la[4] * vz;
+                        lP[4] += la[3] * vx + la[5] * vy;
+                        lP[1] += 2 * la[0] * vx + 2 * la[2] * vy + la[6] * vz;
+                        lP[5] += 2 * la[1] * vx + 2 * la[3] * vz + la[6] * vy;
+                        lP[3] += 2 * la[4] * vy + 2 * la[5] * vz + la[6] * vx;
+                        double lu[3];
+                        lu[0] = 2 * la[0] * pxy + 2 * la[1] * pxz + la[2] * pyy + la[3] * pzz + la[6] * pyz + luP[0] - vx * luQ;
+                        lu[1] = la[0] * pxx + 2 * la[2] * pxy + 2 * la[4] * pyz + la[5] * pzz + la[6] * pxz + luP[1] - vy * luQ;
+                        lu[2] = la[1] * pxx + 2 * la[3] * pxz + la[4] * pyy + 2 * la[5] * pyz + la[6] * pxy + luP[2] - vz * luQ;
+                        double lK = 0;
+                        if (iface) {
+                            if (hd) {
+                                const double i1 = 1 / absF, i3 = i1 * i1 * i1;
+                                const double FF[3] = {Fx, Fy, Fz};
+                                for (int k = 0; k < 3; ++k)
+                                    lF[k * N + id] = Ah * (2 * i1 * sA[k] - FF[k] * i3 * sB - FF[k] * i1 * sBB) +
+                                                     K * (sD[k] * i1 - FF[k] * i3 * sE);
+                                lK = sE * i1;
+                            } else if (absF > 0) {
+                                const double q = -Ah * sBB / absF;
+                                lF[0 * N + id] = q * Fx; lF[1 * N + id] = q * Fy; lF[2 * N + id] = q * Fz;
+                            }
+                        }
+                        const double inv2 = 1 / (rho * rho);
+                        lm[0 * N + id] = l_rhoeq / rho + (l_aR - l_aB) * rb * inv2 + lK * beta * rb * rb * inv2;
+                        lm[1 * N + id] = l_rhoeq / rho - (l_aR - l_aB) * rr * inv2 + lK * beta * rr * rr * inv2;
+                        for (int k = 0; k < 3; ++k) lm[(2 + k) * N + id] = lu[k];
+                        for (int k = 0; k < 6; ++k) lm[(5 + k) * N + id] = lP[k];
+                        a_omega -= l_oms;
+                        a_Ah += l_Ah;
+                    }
+            // moments adjoint: psi gathered from the neighbours' F adjoints, then f(t)
+            for (int z = 1; z <= NZ - 2; ++z)
+                for (int y = 1; y <= NY - 2; ++y)
+                    for (int x = 1; x <= NX - 2; ++x) {
+                        const size_t id = idx(x, y, z);
+                        const double rr = rhor[id], rb = rhob[id], rho = rr + rb;
+                        const double vx = ux[id], vy = uy[id], vz = uz[id];
+                        double lpsi = 0;
+                        for (int j = 1; j < Q; ++j) {
+                            const size_t nid = idx(wrapx(x - CX[j]), wrapy(y - CY[j]), wrapz(z - CZ[j]));
+                            lpsi += double(L.w[j]) *
+                                    (CX[j] * lF[0 * N + nid] + CY[j] * lF[1 * N + nid] + CZ[j] * lF[2 * N + nid]);
+                        }
+                        lpsi /= double(L.cs2);
+                        const double lrr = lm[0 * N + id] + lpsi * 2 * rb / (rho * rho);
+                        const double lrb = lm[1 * N + id] - lpsi * 2 * rr / (rho * rho);
+                        const double lP[6] = {lm[5 * N + id], lm[6 * N + id], lm[7 * N + id],
+                                              lm[8 * N + id], lm[9 * N + id], lm[10 * N + id]};
+                        const double lux = lm[2 * N + id] - rho * (2 * vx * lP[0] + vy * lP[1] + vz * lP[5]);
+                        const double luy = lm[3 * N + id] - rho * (2 * vy * lP[2] + vx * lP[1] + vz * lP[3]);
+                        const double luz = lm[4 * N + id] - rho * (2 * vz * lP[4] + vx * lP[5] + vy * lP[3]);
+                        double lrho = -(lP[0] * vx * vx + lP[1] * vx * vy + lP[2] * vy * vy + lP[3] * vy * vz +
+                                        lP[4] * vz * vz + lP[5] * vx * vz);
+                        lrho -= (lux * vx + luy * vy + luz * vz) / rho;
+                        for (int i = 0; i < Q; ++i) {
+                            const double lgi = lP[0] * L.Hxx[i] + lP[1] * L.Hxy[i] + lP[2] * L.Hyy[i] + lP[3] * L.Hyz[i] +
+                                               lP[4] * L.Hzz[i] + lP[5] * L.Hxz[i] +
+                                               (CX[i] * lux + CY[i] * luy + CZ[i] * luz) / rho + lrho;
+                            nr[fidx(id, i)] = lrr + lgi;
+                            nb[fidx(id, i)] = lrb + lgi;
+                        }
+                    }
+            std::swap(lr, nr);
+            std::swap(lb, nb);
+        }
+        // dJ/du0 of f0 = feq(rho_c, u0); the moments of f(0) are loaded
+        for (size_t k = 0; k < size_t(3) * N; ++k) du0[k] = 0;
+        for (int z = 1; z <= NZ - 2; ++z)
+            for (int y = 1; y <= NY - 2; ++y)
+                for (int x = 1; x <= NX - 2; ++x) {
+                    const size_t id = idx(x, y, z);
+                    const double rr = rhor[id], rb = rhob[id];
+                    const double vx = ux[id], vy = uy[id], vz = uz[id], usq = vx * vx + vy * vy + vz * vz;
+                    double gx = 0, gy = 0, gz = 0, gq = 0;
+                    for (int i = 0; i < Q; ++i) {
+                        const double cu = CX[i] * vx + CY[i] * vy + CZ[i] * vz;
+                        const double P = 1 / double(L.cs2) + cu / double(L.cs4) + cu * cu / (2 * double(L.cs6)) -
+                                         usq / (2 * double(L.cs4));
+                        const double Qd = 1 / double(L.cs2) + cu / double(L.cs4);
+                        const double wl = double(L.w[i]) * (lr[fidx(id, i)] * rr + lb[fidx(id, i)] * rb);
+                        gx += wl * P * CX[i];
+                        gy += wl * P * CY[i];
+                        gz += wl * P * CZ[i];
+                        gq += wl * Qd;
+                    }
+                    du0[id] = gx - vx * gq;
+                    du0[N + id] = gy - vy * gq;
+                    du0[2 * N + id] = gz - vz * gq;
+                }
+        // omega = 1/tau (nu = (tau - 1/2) cs^2), A/2 = sigma / (8 cs^4 tau)
+        const double omega = double(omega_sponge(1)), tau = double(taub);
+        out[0] = Jv;
+        out[1] = a_Ah / (8 * double(L.cs4) * tau);
+        out[2] = a_omega * (-omega * omega) + a_Ah * (-Ah / tau);
+        fr = hr[0];
+        fb = hb[0];
+        step = step0;
+    }
 };
 
 struct Handle {
@@ -612,6 +843,16 @@ void orc_set_fields(void *hv, const double *rr, const double *rb, const double *
     Handle *h = static_cast<Handle *>(hv);
     DISPATCH(h, (copy_in(O.rhor, rr), copy_in(O.rhob, rb), copy_in(O.ux, vx), copy_in(O.uy, vy), copy_in(O.uz, vz)));
 }
+// Discrete adjoint of the periodic box (see Oracle::adjoint_periodic).
+// out: J, dJ/dsigma, dJ/dtau; du0: 3*Ncells.  Returns 0, or -1 if the case is
+// not the periodic box.
+int orc_adjoint_periodic(void *hv, const double *target, int nsteps, double *out, double *du0) {
+    Handle *h = static_cast<Handle *>(hv);
+    int rc = 0;
+    DISPATCH(h, (O.periodic() ? (O.adjoint_periodic(target, nsteps, out, du0), 0) : (rc = -1)));
+    return rc;
+}
+
 // Per-column inlet velocity multipliers (NX*NZ, x fastest); NULL restores the top-hat.
 void orc_set_inlet_profile(void *hv, const double *prof) {
     Handle *h = static_cast<Handle *>(hv);

@@ -37,6 +37,7 @@ def _load():
         "orc_set_fields": ([P, D, D, D, D, D], None),
         "orc_get_fields": ([P, D, D, D, D, D], None),
         "orc_set_inlet_profile": ([P, D], None),
+        "orc_adjoint_periodic": ([P, D, C.c_int, D, D], C.c_int),
         "orc_get_stress": ([P, D], None),
         "orc_macros": ([P], None),
         "orc_collistream": ([P], None),
@@ -118,6 +119,17 @@ class Oracle:
     def set_fields(self, rhor, rhob, ux, uy, uz):
         arrs = [np.ascontiguousarray(a, np.float64).reshape(-1) for a in (rhor, rhob, ux, uy, uz)]
         self.lib.orc_set_fields(self._h, *[_dp(a) for a in arrs])
+
+    def adjoint_periodic(self, target, nsteps: int):
+        """Discrete adjoint of the periodic box from the current state: J =
+        sum (psi_T - target)^2 and dJ/dsigma, dJ/dtau, dJ/du0 ((3, Ncells))."""
+        tgt = np.ascontiguousarray(target, np.float64).reshape(-1)
+        out = np.zeros(3)
+        du0 = np.zeros(3 * self.N)
+        rc = self.lib.orc_adjoint_periodic(self._h, _dp(tgt), int(nsteps), _dp(out), _dp(du0))
+        if rc != 0:
+            raise ValueError("the oracle's adjoint covers the periodic box")
+        return {"J": out[0], "dJ_dsigma": out[1], "dJ_dtau": out[2], "dJ_du0": du0.reshape(3, self.N)}
 
     def set_inlet_profile(self, prof):
         """Per-column inlet velocity multipliers ((NZ, NX) or NX*NZ); None restores the top-hat."""
