@@ -314,6 +314,15 @@ mcg_status mcg_output_open(mcg_handle *h, const char *root_dir);
 /* The NOUTPUT block of main.cu:73-103 for `step`: tke sample (stdout line +
  * tke_*.bin), radial outputs when statistics run, VTI when write_vti_output. */
 mcg_status mcg_output_step(mcg_handle *h, int32_t step);
+/* The same output step without stopping the GPU (no counterpart in the
+ * reference): the solver's stream copies the fields and radial sums to a
+ * device staging slot and sums the kinetic energy; a second stream and a
+ * worker thread download them and write the same files as mcg_output_step, in
+ * step order, while stepping continues.  Two slots: a third call waits for the
+ * oldest.  Synchronous output and tke calls flush first. */
+mcg_status mcg_output_step_async(mcg_handle *h, int32_t step);
+/* Waits for every pending asynchronous output; returns the first write error. */
+mcg_status mcg_output_flush(mcg_handle *h);
 /* write_radial_profile_outputs (meanF/meanFieldsRT.cuh:297-336). */
 mcg_status mcg_write_radial_outputs(mcg_handle *h);
 /* write_vti (io/save_data.cuh:137-200) of the current fields to `path`. */

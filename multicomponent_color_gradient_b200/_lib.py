@@ -98,6 +98,8 @@ SIGNATURES = {
                             _F],
     "mcg_output_open": [_P, C.c_char_p],
     "mcg_output_step": [_P, C.c_int32],
+    "mcg_output_step_async": [_P, C.c_int32],
+    "mcg_output_flush": [_P],
     "mcg_write_radial_outputs": [_P],
     "mcg_write_vti": [_P, C.c_char_p],
     "mcg_write_uy_average": [_P],

@@ -27,13 +27,30 @@ mcg_status cuda_fail(cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? MCG_ERR_OOM : MCG_ERR_CUDA;
 }
 
-void radial_counts(const mcg_handle *h, uint64_t *count) {
+void radial_counts_for(const mcg_handle *h, uint32_t samples, uint64_t *count) {
     const int NY = h->p.NY, NRB = h->p.NX / 2;
     for (int y = 0; y < NY; ++y)
         for (int r = 0; r < NRB; ++r) {
             const bool interior = y >= 1 && y <= NY - 2;
-            count[size_t(y) * NRB + r] = interior ? uint64_t(h->stats_samples) * h->ncols[r] : 0;
+            count[size_t(y) * NRB + r] = interior ? uint64_t(samples) * h->ncols[r] : 0;
         }
+}
+
+void radial_counts(const mcg_handle *h, uint64_t *count) { radial_counts_for(h, h->stats_samples, count); }
+
+StatsSnapshot stats_snapshot(const mcg_handle *h) {
+    StatsSnapshot s;
+    s.started = h->stats_started;
+    s.start_step = h->stats_start_step;
+    s.samples = h->stats_samples;
+    return s;
+}
+
+void tke_update(mcg_handle *h, int32_t step, double total) {
+    h->tke_total = float(total);
+    const unsigned sample_count = unsigned(step) / unsigned(h->p.NOUTPUT);
+    const float count = float(sample_count);
+    h->tke_avg = (h->tke_avg * count + h->tke_total) / (count + 1.0f);
 }
 
 }  // namespace mcg
@@ -138,11 +155,13 @@ size_t pop_buffer_bytes(const mcg_params &p) {
 }
 
 void release(mcg_handle *h) {
+    mcg::async_release(h);
     mcg::io_close(h);
     void *ptrs[] = {h->s.pops[0], h->s.pops[1], h->s.mom,      h->s.psi[0], h->s.psi[1], h->s.radial,
-                    h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar, h->s.bmom,  h->d_inlet_profile};
+                    h->s.uy_avg,  h->s.partials, h->s.flag, h->d_scalar, h->s.bmom,  h->d_inlet_profile, h->d_vti_text};
     for (void *q : ptrs)
         if (q) cudaFree(q);
+    if (h->h_vti_text) cudaFreeHost(h->h_vti_text);
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -723,16 +742,13 @@ mcg_status mcg_get_radial_state(const mcg_handle *h, int32_t *started, uint32_t 
 
 mcg_status mcg_compute_tke(mcg_handle *h, int32_t step, float *tke_total, float *tke_avg) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = mcg::async_flush(h)) return s;  // the worker owns the tke state while outputs are pending
     if (mcg_status s = ensure_moments(h)) return s;
     MCG_LAUNCH(h, mcg::launch_tke(h->s, h->d_scalar, h->stream), "tke kernel");
     double tot = 0;
     MCG_CUDA(cudaMemcpyAsync(&tot, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "download tke");
     MCG_CUDA(cudaStreamSynchronize(h->stream), "tke");
-    // kernels.cu:154-166: running average over output samples, float
-    h->tke_total = float(tot);
-    const unsigned sample_count = unsigned(step) / unsigned(h->p.NOUTPUT);
-    const float count = float(sample_count);
-    h->tke_avg = (h->tke_avg * count + h->tke_total) / (count + 1.0f);
+    mcg::tke_update(h, step, tot);  // kernels.cu:154-166: running average over output samples, float
     if (tke_total) *tke_total = h->tke_total;
     if (tke_avg) *tke_avg = h->tke_avg;
     return MCG_OK;
@@ -791,12 +807,14 @@ mcg_status mcg_output_open(mcg_handle *h, const char *root_dir) {
 
 mcg_status mcg_output_close(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = mcg::async_flush(h)) return s;
     return mcg::io_close(h);
 }
 
 mcg_status mcg_output_step(mcg_handle *h, int32_t step) {
     if (mcg_status s = check_handle(h)) return s;
     if (h->case_dir.empty()) return fail(MCG_ERR_STATE, "mcg_output_open has not been called");
+    if (mcg_status s = mcg::async_flush(h)) return s;
     // main.cu:73-103
     if (mcg_status s = mcg_compute_tke(h, step, nullptr, nullptr)) return s;
     if (mcg_status s = mcg::io_write_tke_sample(h, step)) return s;
@@ -810,14 +828,28 @@ mcg_status mcg_output_step(mcg_handle *h, int32_t step) {
     return MCG_OK;
 }
 
+mcg_status mcg_output_step_async(mcg_handle *h, int32_t step) {
+    if (mcg_status s = check_handle(h)) return s;
+    if (h->case_dir.empty()) return fail(MCG_ERR_STATE, "mcg_output_open has not been called");
+    if (mcg_status s = ensure_moments(h)) return s;
+    return mcg::async_enqueue(h, step);
+}
+
+mcg_status mcg_output_flush(mcg_handle *h) {
+    if (mcg_status s = check_handle(h)) return s;
+    return mcg::async_flush(h);
+}
+
 mcg_status mcg_write_radial_outputs(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = mcg::async_flush(h)) return s;
     if (h->case_dir.empty()) return fail(MCG_ERR_STATE, "mcg_output_open has not been called");
     return mcg::io_write_radial(h);
 }
 
 mcg_status mcg_write_vti(mcg_handle *h, const char *path) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = mcg::async_flush(h)) return s;
     MCG_REQUIRE(path != nullptr, "path is null");
     if (mcg_status s = ensure_moments(h)) return s;
     return mcg::io_write_vti(h, path);
@@ -825,6 +857,7 @@ mcg_status mcg_write_vti(mcg_handle *h, const char *path) {
 
 mcg_status mcg_write_uy_average(mcg_handle *h) {
     if (mcg_status s = check_handle(h)) return s;
+    if (mcg_status s = mcg::async_flush(h)) return s;
     if (h->case_dir.empty()) return fail(MCG_ERR_STATE, "mcg_output_open has not been called");
     return mcg::io_write_uy_average(h);
 }

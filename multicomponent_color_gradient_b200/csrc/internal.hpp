@@ -11,6 +11,17 @@
 #include "../../include/mcg.h"
 #include "kernels.cuh"
 
+namespace mcg {
+// The radial-statistics state an output writes (a copy, so that outputs
+// written on a worker thread see the state of the step they belong to).
+struct StatsSnapshot {
+    bool started = false;
+    uint32_t start_step = 0;
+    uint32_t samples = 0;
+};
+struct AsyncOutput;  // output_async.cpp
+}  // namespace mcg
+
 struct mcg_handle {
     mcg_params p{};
     mcg::DeviceState s{};
@@ -41,6 +52,9 @@ struct mcg_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<cudaEvent_t> prof_events;  // mcg_step_profiled
 
+    mcg::AsyncOutput *async_out = nullptr;  // mcg_output_step_async pipeline (created on first use)
+    char *d_vti_text = nullptr, *h_vti_text = nullptr;  // VTI text of mcg_output_step (first use)
+
     // output files (meanF/meanFieldsRT.cuh:23-33)
     std::string case_dir, mean_dir, vti_dir;
     FILE *f_tke_total = nullptr, *f_tke_avg = nullptr, *f_tke_diff = nullptr;
@@ -54,6 +68,11 @@ mcg_status cuda_fail(cudaError_t e, const char *what);
 
 // Radial count materialisation: samples * ncols[rb] on interior y rows.
 void radial_counts(const mcg_handle *h, uint64_t *count);
+void radial_counts_for(const mcg_handle *h, uint32_t samples, uint64_t *count);
+StatsSnapshot stats_snapshot(const mcg_handle *h);
+// kernels.cu:154-166 running average of the total kinetic energy, from the
+// float64 device sum of this output step
+void tke_update(mcg_handle *h, int32_t step, double total);
 
 // io.cpp
 mcg_status io_open(mcg_handle *h, const char *root);
@@ -62,7 +81,16 @@ mcg_status io_write_case_metadata(mcg_handle *h);
 mcg_status io_write_radial(mcg_handle *h);
 mcg_status io_write_vti(mcg_handle *h, const std::string &path);
 mcg_status io_write_tke_sample(mcg_handle *h, int32_t step);
+// The same writers on host copies: radial sums [5][NY*NR_BINS], fields
+// [5][Ncells] (rhor, rhob, ux, uy, uz), the statistics state of the output step.
+mcg_status io_write_radial_host(mcg_handle *h, const StatsSnapshot &st, const double *sums);
+// text: the four base64 arrays laid out by vti_text_layout (launch_vti_encode).
+mcg_status io_write_vti_text(mcg_handle *h, const std::string &path, const char *text);
+mcg_status io_write_tke_sample_snap(mcg_handle *h, int32_t step, const StatsSnapshot &st);
+// Asynchronous outputs (output_async.cpp): wait for pending writes; release.
+mcg_status async_flush(mcg_handle *h);
+mcg_status async_enqueue(mcg_handle *h, int32_t step);
+void async_release(mcg_handle *h);
 mcg_status io_write_uy_average(mcg_handle *h);
-std::string base64_encode(const unsigned char *data, size_t len);
 
 }  // namespace mcg

@@ -30,47 +30,6 @@ bool write_binary(const std::string &path, const void *data, size_t elem, size_t
 
 int round_int(float v) { return static_cast<int>(std::lround(double(v))); }
 
-mcg_status download_fields(mcg_handle *h, std::vector<float> &buf) {
-    const size_t N = h->s.g.N;
-    buf.resize(5 * N);
-    cudaError_t e = cudaMemcpyAsync(buf.data(), h->s.mom, 5 * N * 4, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) return cuda_fail(e, "download fields");
-    return MCG_OK;
-}
-
-}  // namespace
-
-std::string base64_encode(const unsigned char *data, size_t len) {
-    static const char tbl[] = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
-    std::string out((len + 2) / 3 * 4, '=');
-    size_t o = 0, i = 0;
-    for (; i + 2 < len; i += 3) {
-        const uint32_t v = (uint32_t(data[i]) << 16) | (uint32_t(data[i + 1]) << 8) | uint32_t(data[i + 2]);
-        out[o++] = tbl[(v >> 18) & 63];
-        out[o++] = tbl[(v >> 12) & 63];
-        out[o++] = tbl[(v >> 6) & 63];
-        out[o++] = tbl[v & 63];
-    }
-    if (i < len) {
-        const uint32_t b1 = (i + 1 < len) ? data[i + 1] : 0;
-        const uint32_t v = (uint32_t(data[i]) << 16) | (b1 << 8);
-        out[o++] = tbl[(v >> 18) & 63];
-        out[o++] = tbl[(v >> 12) & 63];
-        if (i + 1 < len) out[o++] = tbl[(v >> 6) & 63];
-    }
-    return out;
-}
-
-namespace {
-// [UInt64 byte count][payload], base64 (VTK XML binary, header_type UInt64)
-std::string vtk_block(const std::vector<unsigned char> &payload) {
-    std::vector<unsigned char> buf(8 + payload.size());
-    const uint64_t n = payload.size();
-    std::memcpy(buf.data(), &n, 8);
-    if (!payload.empty()) std::memcpy(buf.data() + 8, payload.data(), payload.size());
-    return base64_encode(buf.data(), buf.size());
-}
 }  // namespace
 
 mcg_status io_open(mcg_handle *h, const char *root) {
@@ -129,7 +88,7 @@ mcg_status io_write_case_metadata(mcg_handle *h) {
     return MCG_OK;
 }
 
-static mcg_status write_radial_metadata(mcg_handle *h) {
+static mcg_status write_radial_metadata(mcg_handle *h, const StatsSnapshot &st) {
     const mcg_params &p = h->p;
     const std::string path = h->mean_dir + "/radial_profile_metadata.txt";
     FILE *f = std::fopen(path.c_str(), "w");
@@ -150,14 +109,14 @@ static mcg_status write_radial_metadata(mcg_handle *h) {
     std::fprintf(f, "U_jet %.9g\n", double(p.jet_velocity));
     std::fprintf(f, "jet_radius %.9g\n", double(p.jet_radius));
     std::fprintf(f, "jet_velocity %.9g\n", double(p.jet_velocity));
-    std::fprintf(f, "uy_avg_started %d\n", h->stats_started ? 1 : 0);
-    std::fprintf(f, "start_step %u\n", h->stats_start_step);
-    std::fprintf(f, "uy_avg_start_step %u\n", h->stats_start_step);
-    std::fprintf(f, "uy_avg_samples %u\n", h->stats_samples);
-    std::fprintf(f, "radial_sample_count %u\n", h->stats_samples);
-    if (h->stats_started && h->stats_samples > 0) {
-        std::fprintf(f, "uy_avg_first_sample_step %u\n", h->stats_start_step);
-        std::fprintf(f, "uy_avg_last_sample_step %u\n", h->stats_start_step + h->stats_samples - 1);
+    std::fprintf(f, "uy_avg_started %d\n", st.started ? 1 : 0);
+    std::fprintf(f, "start_step %u\n", st.start_step);
+    std::fprintf(f, "uy_avg_start_step %u\n", st.start_step);
+    std::fprintf(f, "uy_avg_samples %u\n", st.samples);
+    std::fprintf(f, "radial_sample_count %u\n", st.samples);
+    if (st.started && st.samples > 0) {
+        std::fprintf(f, "uy_avg_first_sample_step %u\n", st.start_step);
+        std::fprintf(f, "uy_avg_last_sample_step %u\n", st.start_step + st.samples - 1);
     }
     const bool ok = std::ferror(f) == 0;
     if (std::fclose(f) != 0 || !ok) return fail(MCG_ERR_IO, "short write " + path);
@@ -165,49 +124,50 @@ static mcg_status write_radial_metadata(mcg_handle *h) {
 }
 
 mcg_status io_write_radial(mcg_handle *h) {
-    if (!h->stats_started || h->stats_samples == 0) return write_radial_metadata(h);
+    const StatsSnapshot st = stats_snapshot(h);
+    if (!st.started || st.samples == 0) return write_radial_metadata(h, st);
     const size_t M = size_t(h->p.NY) * (h->p.NX / 2);
     std::vector<double> sums(5 * M);
-    std::vector<uint64_t> count(M);
     cudaError_t e = cudaMemcpyAsync(sums.data(), h->s.radial, 5 * M * 8, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(e, "download radial sums");
-    radial_counts(h, count.data());
+    return io_write_radial_host(h, st, sums.data());
+}
+
+mcg_status io_write_radial_host(mcg_handle *h, const StatsSnapshot &st, const double *sums) {
+    if (!st.started || st.samples == 0) return write_radial_metadata(h, st);
+    const size_t M = size_t(h->p.NY) * (h->p.NX / 2);
+    std::vector<uint64_t> count(M);
+    radial_counts_for(h, st.samples, count.data());
     static const char *names[5] = {"radial_sum_uy.bin", "radial_sum_uy2.bin", "radial_sum_ur.bin",
                                    "radial_sum_ur2.bin", "radial_sum_uruy.bin"};
     bool ok = true;
-    for (int k = 0; k < 5; ++k) ok = write_binary(h->mean_dir + "/" + names[k], sums.data() + k * M, 8, M) && ok;
+    for (int k = 0; k < 5; ++k) ok = write_binary(h->mean_dir + "/" + names[k], sums + k * M, 8, M) && ok;
     ok = write_binary(h->mean_dir + "/radial_count.bin", count.data(), 8, M) && ok;
-    if (mcg_status s = write_radial_metadata(h)) return s;
+    if (mcg_status s = write_radial_metadata(h, st)) return s;
     if (!ok) return fail(MCG_ERR_IO, "short write in " + h->mean_dir);
     return MCG_OK;
 }
 
+// The VTI text is encoded on the device from the moment planes
+// (launch_vti_encode) and downloaded once; the host only writes it.
 mcg_status io_write_vti(mcg_handle *h, const std::string &path) {
-    std::vector<float> f;
-    if (mcg_status s = download_fields(h, f)) return s;
-    const size_t N = h->s.g.N;
-    const float *rr = f.data(), *rb = rr + N, *ux = rb + N, *uy = ux + N, *uz = uy + N;
-    std::vector<unsigned char> pl(N * 4);
-    std::memcpy(pl.data(), rr, N * 4);
-    const std::string e_rr = vtk_block(pl);
-    std::memcpy(pl.data(), rb, N * 4);
-    const std::string e_rb = vtk_block(pl);
-    {
-        float *q = reinterpret_cast<float *>(pl.data());
-        for (size_t i = 0; i < N; ++i) q[i] = rr[i] + rb[i];
+    const VtiText L = vti_text_layout(uint64_t(h->s.g.N));
+    cudaError_t e = cudaSuccess;
+    if (!h->d_vti_text) e = cudaMalloc(&h->d_vti_text, L.total);
+    if (e == cudaSuccess && !h->h_vti_text) e = cudaMallocHost(&h->h_vti_text, L.total);
+    if (e == cudaSuccess) {
+        e = launch_vti_encode(h->s, h->d_vti_text, h->stream);
+        if (e == cudaSuccess) ++h->launches;
     }
-    const std::string e_rho = vtk_block(pl);
-    std::vector<unsigned char> pu(3 * N * 4);
-    {
-        float *q = reinterpret_cast<float *>(pu.data());
-        for (size_t i = 0; i < N; ++i) {
-            q[3 * i] = ux[i];
-            q[3 * i + 1] = uy[i];
-            q[3 * i + 2] = uz[i];
-        }
-    }
-    const std::string e_u = vtk_block(pu);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->h_vti_text, h->d_vti_text, L.total, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "VTI text");
+    return io_write_vti_text(h, path, h->h_vti_text);
+}
+
+mcg_status io_write_vti_text(mcg_handle *h, const std::string &path, const char *text) {
+    const VtiText L = vti_text_layout(uint64_t(h->s.g.N));
     FILE *out = std::fopen(path.c_str(), "wb");
     if (!out) return fail(MCG_ERR_IO, "cannot open " + path);
     const int X = h->p.NX - 1, Y = h->p.NY - 1, Z = h->p.NZ - 1;
@@ -216,15 +176,13 @@ mcg_status io_write_vti(mcg_handle *h, const std::string &path) {
     std::fprintf(out, "  <ImageData WholeExtent=\"0 %d 0 %d 0 %d\" Origin=\"0 0 0\" Spacing=\"1 1 1\">\n", X, Y, Z);
     std::fprintf(out, "    <Piece Extent=\"0 %d 0 %d 0 %d\">\n", X, Y, Z);
     std::fprintf(out, "      <PointData Scalars=\"rhor\" Vectors=\"u\">\n");
-    const std::pair<const char *, const std::string *> arrays[3] = {{"rhor", &e_rr}, {"rhob", &e_rb}, {"rho", &e_rho}};
-    for (const auto &a : arrays) {
-        std::fprintf(out, "        <DataArray type=\"Float32\" Name=\"%s\" format=\"binary\">\n", a.first);
-        std::fwrite(a.second->data(), 1, a.second->size(), out);
+    static const char *names[4] = {"rhor", "rhob", "rho", "u"};
+    for (int a = 0; a < 4; ++a) {
+        std::fprintf(out, "        <DataArray type=\"Float32\" Name=\"%s\"%s format=\"binary\">\n", names[a],
+                     a == 3 ? " NumberOfComponents=\"3\"" : "");
+        std::fwrite(text + L.off[a], 1, L.len[a], out);
         std::fprintf(out, "\n        </DataArray>\n");
     }
-    std::fprintf(out, "        <DataArray type=\"Float32\" Name=\"u\" NumberOfComponents=\"3\" format=\"binary\">\n");
-    std::fwrite(e_u.data(), 1, e_u.size(), out);
-    std::fprintf(out, "\n        </DataArray>\n");
     std::fprintf(out, "      </PointData>\n      <CellData>\n      </CellData>\n    </Piece>\n  </ImageData>\n</VTKFile>\n");
     const bool ok = std::ferror(out) == 0;
     if (std::fclose(out) != 0 || !ok) return fail(MCG_ERR_IO, "short write " + path);
@@ -233,6 +191,10 @@ mcg_status io_write_vti(mcg_handle *h, const std::string &path) {
 
 // update_tke_state + write_tke_outputs (meanF/meanFieldsRT.cuh:192-227, 366-381)
 mcg_status io_write_tke_sample(mcg_handle *h, int32_t step) {
+    return io_write_tke_sample_snap(h, step, stats_snapshot(h));
+}
+
+mcg_status io_write_tke_sample_snap(mcg_handle *h, int32_t step, const StatsSnapshot &st) {
     if (h->first_tke) {
         h->tke_delta = 0.f;
         h->tke_abs_delta = 0.f;
@@ -243,9 +205,9 @@ mcg_status io_write_tke_sample(mcg_handle *h, int32_t step) {
     }
     std::cout << std::scientific << "step " << step << " | tke_prev = " << h->tke_avg_prev
               << " | tke_avg = " << h->tke_avg << " | delta_tke_avg = " << h->tke_abs_delta;
-    if (h->stats_started)
-        std::cout << " | uy_radial_avg = on | uy_avg_start_step = " << h->stats_start_step
-                  << " | uyavg_samples = " << h->stats_samples << " | radial_count = on";
+    if (st.started)
+        std::cout << " | uy_radial_avg = on | uy_avg_start_step = " << st.start_step
+                  << " | uyavg_samples = " << st.samples << " | radial_count = on";
     else
         std::cout << " | uy_radial_avg = waiting | uyavg_samples = 0";
     std::cout << "\n";

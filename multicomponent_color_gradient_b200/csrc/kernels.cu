@@ -2093,6 +2093,64 @@ cudaError_t launch_uy_average(const DeviceState &s, uint32_t samples, cudaStream
     return cudaGetLastError();
 }
 
+// ---- VTI text (base64, RFC 4648 alphabet, '=' padding) ----------------------
+
+__device__ __forceinline__ uint32_t b64_char(uint32_t v) {
+    return v < 26 ? 'A' + v : v < 52 ? 'a' + (v - 26) : v < 62 ? '0' + (v - 52) : v == 62 ? '+' : '/';
+}
+
+// Word e of array a's float32 payload.
+__device__ __forceinline__ uint32_t vti_word(const float *__restrict__ m, uint64_t N, int a, uint64_t e) {
+    if (a < 2) return __float_as_uint(m[a * N + e]);
+    if (a == 2) return __float_as_uint(__fadd_rn(m[e], m[N + e]));
+    const uint64_t node = e / 3;
+    return __float_as_uint(m[(2 + (e - 3 * node)) * N + node]);
+}
+
+// One thread per 3-byte group of [count][payload] -> one 4-character word.
+// blockIdx.y selects the array; stores are 4-byte words, coalesced per warp.
+__global__ void __launch_bounds__(256) k_vti_encode(const float *__restrict__ m, uint64_t N, char *__restrict__ text,
+                                                    VtiText L) {
+    const int a = blockIdx.y;
+    const uint64_t payload = (a == 3 ? 3 : 1) * N * 4, total = payload + 8, groups = (total + 2) / 3;
+    uint32_t *out = reinterpret_cast<uint32_t *>(text + L.off[a]);
+    for (uint64_t g = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; g < groups;
+         g += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t v = 0, cw = 0;
+        uint64_t ce = ~uint64_t(0);
+        for (int k = 0; k < 3; ++k) {
+            const uint64_t p = 3 * g + k;
+            uint32_t b = 0;
+            if (p < 8) {
+                b = uint32_t(payload >> (8 * p)) & 0xffu;
+            } else if (p < total) {
+                const uint64_t q = p - 8, e = q >> 2;
+                if (e != ce) {
+                    ce = e;
+                    cw = vti_word(m, N, a, e);
+                }
+                b = (cw >> (8 * (q & 3))) & 0xffu;
+            }
+            v = (v << 8) | b;
+        }
+        const uint64_t rest = total - 3 * g;
+        const uint32_t valid = rest >= 3 ? 4u : uint32_t(rest) + 1u;  // characters that carry data
+        uint32_t w = 0;
+        for (uint32_t c = 0; c < 4; ++c) w |= (c < valid ? b64_char((v >> (18 - 6 * c)) & 63u) : uint32_t('=')) << (8 * c);
+        out[g] = w;
+    }
+}
+
+cudaError_t launch_vti_encode(const DeviceState &s, char *text, cudaStream_t st) {
+    const uint64_t N = uint64_t(s.g.N);
+    const VtiText L = vti_text_layout(N);
+    const uint64_t groups = (8 + 3 * N * 4 + 2) / 3;
+    const uint64_t want = (groups + 255) / 256;
+    const unsigned bx = unsigned(want < uint64_t(8 * 148) ? want : uint64_t(8 * 148));
+    k_vti_encode<<<dim3(bx, 4), 256, 0, st>>>(s.mom, N, text, L);
+    return cudaGetLastError();
+}
+
 uint32_t conservation_blocks(const Geometry &g) {
     const size_t want = (size_t(g.N) + kRedThreads - 1) / kRedThreads;
     return uint32_t(want < size_t(kConsBlocksMax) ? want : size_t(kConsBlocksMax));

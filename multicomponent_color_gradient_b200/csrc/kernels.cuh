@@ -136,6 +136,29 @@ cudaError_t launch_gather_pops(const DeviceState &s, int cur, float *fr_ref, flo
 // Diagnostics / mean fields.
 cudaError_t launch_tke(const DeviceState &s, double *out, cudaStream_t st);
 cudaError_t launch_uy_average(const DeviceState &s, uint32_t samples, cudaStream_t st);
+
+// VTK XML image data, format="binary" (io/save_data.cuh:137-215): each array is
+// the base64 text of [UInt64 byte count][little-endian float32 payload].  The
+// four arrays are rhor, rhob, rho = rhor + rhob and u (ux, uy, uz interleaved
+// per node); their texts lie back to back in one buffer.
+struct VtiText {
+    uint64_t len[4], off[4], total;
+};
+inline VtiText vti_text_layout(uint64_t N) {
+    VtiText t{};
+    uint64_t at = 0;
+    for (int a = 0; a < 4; ++a) {
+        const uint64_t bytes = 8 + (a == 3 ? 3 : 1) * N * 4;
+        t.len[a] = (bytes + 2) / 3 * 4;
+        t.off[a] = at;
+        at += t.len[a];
+    }
+    t.total = at;
+    return t;
+}
+// Encodes the first five moment planes of s.mom ([5][N]: rr, rb, ux, uy, uz)
+// into text (vti_text_layout(N).total bytes, 4-byte aligned).
+cudaError_t launch_vti_encode(const DeviceState &s, char *text, cudaStream_t st);
 // Float64 sums over interior nodes of f(t): mass r, mass b, momentum x,y,z.
 // partials: scratch of at least conservation_blocks(g)*5 doubles.
 uint32_t conservation_blocks(const Geometry &g);

@@ -284,6 +284,13 @@ class Solver:
     def output_step(self, step: int) -> None:
         self._c("mcg_output_step", int(step))
 
+    def output_step_async(self, step: int) -> None:
+        """mcg_output_step without stopping the GPU; files appear after output_flush."""
+        self._c("mcg_output_step_async", int(step))
+
+    def output_flush(self) -> None:
+        self._c("mcg_output_flush")
+
     def write_radial_outputs(self) -> None:
         self._c("mcg_write_radial_outputs")
 

@@ -46,7 +46,8 @@ def decode_vti(path):
     arrays = {}
     for m in re.finditer(r'<DataArray type="Float32" Name="(\w+)"(?: NumberOfComponents="3")? format="binary">\n'
                          r'([A-Za-z0-9+/=]+)\n        </DataArray>', text):
-        raw = base64.b64decode(m.group(2))
+        raw = base64.b64decode(m.group(2), validate=True)
+        assert base64.b64encode(raw).decode() == m.group(2)  # canonical text, '=' padding
         n = struct.unpack("<Q", raw[:8])[0]
         assert n == len(raw) - 8
         arrays[m.group(1)] = np.frombuffer(raw[8:], np.float32)
@@ -126,3 +127,43 @@ def test_cpp_driver_runs_the_main_loop(tmp_path):
     mean = tmp_path / "JET_VTK" / "Re45_We3" / "mean_profiles"
     assert (mean / "radial_sum_uy.bin").stat().st_size == 40 * 12 * 8
     assert (tmp_path / "JET_VTK" / "Re45_We3" / "vti_data" / "lbm_00000100.vti").exists()
+
+
+def _run_outputs(root, asynchronous):
+    case = get_case("jet_24x40x24", NOUTPUT=20, NSTATS_START_STEP=10, write_vti_output=1, NSTEP=61)
+    with Solver(case) as S:
+        S.output_open(str(root))
+        S.init_jet()
+        for step in range(61):
+            S.step(1)
+            if step % case["NOUTPUT"] == 0:
+                S.output_step_async(step) if asynchronous else S.output_step(step)
+        if asynchronous:
+            S.output_flush()
+        S.write_radial_outputs()
+        case_dir, _, _ = S.output_dirs()
+    return case_dir
+
+
+def test_async_outputs_equal_sync_outputs(tmp_path):
+    """mcg_output_step_async writes the same files as mcg_output_step (tke,
+    radial sums and metadata, VTI) while stepping on.  The fields, VTI text and
+    metadata are deterministic and compared byte for byte.  The radial sums
+    and the kinetic energy are float64 atomic sums whose order changes from
+    run to run, so those files are compared within a reordering tolerance."""
+    a = _run_outputs(tmp_path / "sync", False)
+    b = _run_outputs(tmp_path / "async", True)
+    files_a = sorted(os.path.relpath(os.path.join(d, f), a) for d, _, fs in os.walk(a) for f in fs)
+    files_b = sorted(os.path.relpath(os.path.join(d, f), b) for d, _, fs in os.walk(b) for f in fs)
+    assert files_a == files_b and len(files_a) > 10
+    for f in files_a:
+        fa, fb = os.path.join(a, f), os.path.join(b, f)
+        name = os.path.basename(f)
+        if name.startswith("radial_sum_"):
+            x, y = np.fromfile(fa, np.float64), np.fromfile(fb, np.float64)
+            assert x.shape == y.shape and np.max(np.abs(x - y)) <= 1e-10 * max(np.max(np.abs(x)), 1e-30), f
+        elif name.startswith("tke_"):
+            x, y = np.fromfile(fa, np.float32), np.fromfile(fb, np.float32)
+            np.testing.assert_allclose(x, y, rtol=1e-6, atol=1e-12, err_msg=f)
+        else:
+            assert open(fa, "rb").read() == open(fb, "rb").read(), f
