@@ -86,6 +86,7 @@ struct FusedTiling {
     int prefetch;  // planes ahead whose source rows are prefetched into L2 (0: off)
     int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
     int pipe;      // software-pipelined march (k_fused_pipe): one barrier per plane
+    int fixed_nx;  // row length the kernel is compiled for (0: runtime geometry)
 };
 
 struct DeviceState {
