@@ -51,13 +51,14 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(cells: int):
-    """DRAM bytes (read + write) of one k_fused launch scaled from the committed
-    ncu summary (profiles/k_fused_*.md, line `dram_bytes_per_node: <value>`), or None."""
+def traffic_per_launch(cells: int, kernel: str):
+    """DRAM bytes (read + write) of one launch of `kernel` scaled from its
+    committed ncu summary (profiles/<kernel>_jet_*.md, line
+    `dram_bytes_per_node: <value>`), or None."""
     import glob
     import re
 
-    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "k_fused_*.md"))):
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_jet_*.md"))):
         m = re.search(r"dram_bytes_per_node:\s*([0-9.]+)", open(path).read())
         if m:
             return int(float(m.group(1)) * cells)
@@ -323,11 +324,14 @@ def main():
     t_bc = per_kernel["boundary"] / args.steps
     ach = step_bytes * cells / (t_fused * 1e-3) / 1e9
     step_gbps = step_bytes * cells / (ms / args.steps * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_fused", "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "peak_kind": peak_kind, "traffic": traffic_per_launch(cells),
+    tiling = S.tiling()
+    kname = "k_fused_pipe" if tiling["pipelined"] else "k_fused"  # the fused-step kernel that ran
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(ach / hbm_peak, 4), "peak_kind": peak_kind, "traffic": traffic_per_launch(cells, kname),
                 "algorithmic_bytes_per_node": step_bytes,
                 "step_achieved": round(step_gbps, 1), "step_frac": round(step_gbps / hbm_peak, 4),
-                "kernels": {"k_fused": {"ms_per_launch": round(t_fused, 6)},
+                "tiling": tiling,
+                "kernels": {kname: {"ms_per_launch": round(t_fused, 6)},
                             "k_boundary": {"ms_per_launch": round(t_bc, 6)}}}
 
     # end to end through the public API: host state in, K steps, fields out

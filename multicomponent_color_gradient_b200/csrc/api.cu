@@ -501,6 +501,15 @@ mcg_status mcg_set_inlet_bessel(mcg_handle *h, const float *coeffs, int32_t n) {
     return MCG_OK;
 }
 
+mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out) {
+    if (mcg_status s = check_handle(h)) return s;
+    MCG_REQUIRE(out != nullptr, "out is null");
+    const mcg::FusedTiling &t = h->tiling;
+    const int32_t v[MCG_TILING_FIELDS] = {t.ty, t.lz, t.tpr, t.ny_tiles, t.nz_chunks, t.smem_bytes, t.pipe, t.fixed_nx};
+    for (int k = 0; k < MCG_TILING_FIELDS; ++k) out[k] = v[k];
+    return MCG_OK;
+}
+
 mcg_status mcg_get_inlet_profile(mcg_handle *h, float *profile) {
     if (mcg_status s = check_handle(h)) return s;
     MCG_REQUIRE(profile != nullptr, "profile is null");

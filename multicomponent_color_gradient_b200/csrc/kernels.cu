@@ -333,6 +333,22 @@ __constant__ int c_cz[kQ] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0, 0, -1,
 
 // ------------------------------------------------------------------ per-node pieces
 
+// First of the opposite pairs (i, i+1), i = 2p+1, whose direction has a
+// nonzero c_a c_b (a == b: c_a != 0); the moment sums start there.
+__host__ __device__ constexpr int dir_comp(int i, int a) { return a == 0 ? dir_cx(i) : (a == 1 ? dir_cy(i) : dir_cz(i)); }
+__host__ __device__ constexpr int first_pair(int a, int b) {
+    for (int p = 0; p < (kQ - 1) / 2; ++p)
+        if (dir_comp(2 * p + 1, a) * dir_comp(2 * p + 1, b) != 0) return p;
+    return (kQ - 1) / 2;
+}
+template <bool kFirst>
+__device__ __forceinline__ void moment_add(float &acc, float v) {
+    if constexpr (kFirst)
+        acc = v;
+    else
+        acc += v;
+}
+
 // One pulled direction as the pair the colour sums add: (fr, fb), or
 // (fr + fb, fr - fb) for C::kSumDiff; `gi` is the total fr + fb.
 template <class C, int I, class Map>
@@ -373,11 +389,9 @@ __device__ __forceinline__ void pull_densities_from(const Map &pm, const C &code
 // (lbm.cuh:106-164: densities, velocity, second-order Hermite moments minus
 // the equilibrium part).  The loads are issued in direction-index order
 // (measured: issuing them group by group was 5-20 % slower) into registers;
-// the raw moments sum_i c_ia c_ib g_i are then sum-factorised: per (cy, cz)
-// group, s0 = g- + g0 + g+, s1 = g+ - g-, s2 = g+ + g- (sums of 1, cx, cx^2);
-// per cz the groups fold into sums weighted by 1, cy, cy^2; the planes then
-// fold with 1, cz, cz^2.  About 70 adds instead of one multiply-add per
-// direction and moment.
+// the moments are then formed from the sums and differences of opposite
+// pairs, about 100 operations instead of one multiply-add per direction and
+// moment.
 template <class C, class Map>
 __device__ __forceinline__ NodeMoments pull_moments_from(const Map &pm, const C &codec, int x) {
     float2 sum = make_float2(0.f, 0.f);  // (sum fr, sum fb); C::kSumDiff: (sum fr+fb, sum fr-fb)
@@ -386,63 +400,33 @@ __device__ __forceinline__ NodeMoments pull_moments_from(const Map &pm, const C 
         constexpr int i = decltype(I)::value;
         sum = __fadd2_rn(sum, pull_pair<C, i>(pm, codec, x, gv[i]));
     });
-    // raw moments: J = sum c g, Q = sum c c g
-    float Jx, Jy, Jz, Qxx, Qyy, Qzz, Qxy, Qxz, Qyz;
-    static_for<3>([&](auto CZ) {
-        constexpr int cz = decltype(CZ)::value - 1;
-        // sums over the plane cz weighted by 1, cy, cy^2, cx, cx cy, cx^2
-        float t0, ty, tyy, tx, txy, txx;
-        static_for<3>([&](auto CY) {
-            constexpr int cy = decltype(CY)::value - 1;
-            const float gm = gv[dir_of(-1, cy, cz)], g0 = gv[dir_of(0, cy, cz)], gp = gv[dir_of(1, cy, cz)];
-            const float s2 = gp + gm, s0 = s2 + g0, s1 = gp - gm;
-            if constexpr (cy == -1) {
-                t0 = s0;
-                ty = -s0;
-                tyy = s0;
-                tx = s1;
-                txy = -s1;
-                txx = s2;
-            } else if constexpr (cy == 0) {
-                t0 += s0;
-                tx += s1;
-                txx += s2;
-            } else {
-                t0 += s0;
-                ty += s0;
-                tyy += s0;
-                tx += s1;
-                txy += s1;
-                txx += s2;
-            }
-        });
-        if constexpr (cz == -1) {
-            Jz = -t0;
-            Qzz = t0;
-            Jy = ty;
-            Qyz = -ty;
-            Qyy = tyy;
-            Jx = tx;
-            Qxz = -tx;
-            Qxy = txy;
-            Qxx = txx;
-        } else if constexpr (cz == 0) {
-            Jy += ty;
-            Qyy += tyy;
-            Jx += tx;
-            Qxy += txy;
-            Qxx += txx;
-        } else {
-            Jz += t0;
-            Qzz += t0;
-            Jy += ty;
-            Qyz += ty;
-            Qyy += tyy;
-            Jx += tx;
-            Qxz += tx;
-            Qxy += txy;
-            Qxx += txx;
-        }
+    // Moments over the 13 opposite pairs (i, i+1), i odd: d = g_i - g_opp
+    // carries the first moments, s = g_i + g_opp the second.  Near equilibrium
+    // the two members of a pair are within a factor of two, so d is exact and
+    // the momentum sums add small numbers.  The diagonal stresses take s times
+    // the Hermite constants H_aa = c_a^2 - cs^2 (multiply-adds, as lbm.cuh
+    // forms them): the rounding of the two constants cancels at rest, whereas
+    // sum c_a^2 g - rho * float(1/3) is biased by 1e-8 rho at every node and
+    // step, which accumulated to 3x the float32 error of the reference's
+    // arithmetic in the kinetic energy.  (Summing whole (cy, cz) groups
+    // before differencing lost digits of the momentum.)
+    float Jx, Jy, Jz, Qxy, Qxz, Qyz;
+    float Axx = gv[0] * Dir<0>::Hxx, Ayy = gv[0] * Dir<0>::Hyy, Azz = gv[0] * Dir<0>::Hzz;
+    static_for<(kQ - 1) / 2>([&](auto P) {
+        constexpr int p = decltype(P)::value, i = 2 * p + 1;
+        using D = Dir<i>;
+        static_assert(Dir<i + 1>::cx == -D::cx && Dir<i + 1>::cy == -D::cy && Dir<i + 1>::cz == -D::cz,
+                      "directions i, i+1 (i odd) are opposite");
+        const float d = gv[i] - gv[i + 1], sp = gv[i] + gv[i + 1];
+        if constexpr (D::cx != 0) moment_add<p == first_pair(0, 0)>(Jx, D::cx > 0 ? d : -d);
+        if constexpr (D::cy != 0) moment_add<p == first_pair(1, 1)>(Jy, D::cy > 0 ? d : -d);
+        if constexpr (D::cz != 0) moment_add<p == first_pair(2, 2)>(Jz, D::cz > 0 ? d : -d);
+        Axx = fmaf(sp, D::Hxx, Axx);
+        Ayy = fmaf(sp, D::Hyy, Ayy);
+        Azz = fmaf(sp, D::Hzz, Azz);
+        if constexpr (D::cx * D::cy != 0) moment_add<p == first_pair(0, 1)>(Qxy, D::cx * D::cy > 0 ? sp : -sp);
+        if constexpr (D::cx * D::cz != 0) moment_add<p == first_pair(0, 2)>(Qxz, D::cx * D::cz > 0 ? sp : -sp);
+        if constexpr (D::cy * D::cz != 0) moment_add<p == first_pair(1, 2)>(Qyz, D::cy * D::cz > 0 ? sp : -sp);
     });
     float sumr = sum.x, sumb = sum.y;
     if constexpr (C::kSumDiff) {
@@ -452,17 +436,16 @@ __device__ __forceinline__ NodeMoments pull_moments_from(const Map &pm, const C 
     NodeMoments m;
     const float rho = sumr + sumb;
     const float inv = 1.0f / rho;
-    const float rcs2 = rho * kCs2;  // sum g H_aa = Q_aa - cs^2 rho
     m.rr = sumr;
     m.rb = sumb;
     m.ux = Jx * inv;
     m.uy = Jy * inv;
     m.uz = Jz * inv;
-    m.pxx = (Qxx - rcs2) - rho * m.ux * m.ux;
+    m.pxx = Axx - rho * m.ux * m.ux;
     m.pxy = Qxy - rho * m.ux * m.uy;
-    m.pyy = (Qyy - rcs2) - rho * m.uy * m.uy;
+    m.pyy = Ayy - rho * m.uy * m.uy;
     m.pyz = Qyz - rho * m.uy * m.uz;
-    m.pzz = (Qzz - rcs2) - rho * m.uz * m.uz;
+    m.pzz = Azz - rho * m.uz * m.uz;
     m.pxz = Qxz - rho * m.ux * m.uz;
     return m;
 }
