@@ -167,3 +167,29 @@ def test_async_outputs_equal_sync_outputs(tmp_path):
             np.testing.assert_allclose(x, y, rtol=1e-6, atol=1e-12, err_msg=f)
         else:
             assert open(fa, "rb").read() == open(fb, "rb").read(), f
+
+
+def test_async_output_reports_a_writer_error_once(tmp_path):
+    """A file the worker thread cannot write (here: the VTI directory removed
+    after mcg_output_open) comes back from mcg_output_flush as an I/O error;
+    the next flush is clean and later output steps write again."""
+    import shutil
+
+    from multicomponent_color_gradient_b200._lib import McgError
+
+    case = get_case("jet_24x40x24", NOUTPUT=20, NSTATS_START_STEP=10, write_vti_output=1, NSTEP=61)
+    with Solver(case) as S:
+        S.output_open(str(tmp_path))
+        _, _, vti_dir = S.output_dirs()
+        S.init_jet()
+        S.step(5)
+        shutil.rmtree(vti_dir)
+        S.output_step_async(5)
+        with pytest.raises(McgError, match="vti"):
+            S.output_flush()
+        S.output_flush()  # the error was reported once
+        os.makedirs(vti_dir)
+        S.step(5)
+        S.output_step_async(10)
+        S.output_flush()
+        assert os.path.exists(os.path.join(vti_dir, "lbm_00000010.vti"))
