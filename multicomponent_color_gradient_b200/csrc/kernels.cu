@@ -71,11 +71,17 @@ struct CodecF32 {
         r = __ldg(rd + grow + size_t(0 * 3 + dir_cx(I) + 1) * NX + xs);
         b = __ldg(rd + grow + size_t(1 * 3 + dir_cx(I) + 1) * NX + xs);
     }
-    // pull through `p` = the source node's red slot of direction I
+    // pull in two halves: the raw words at `p` = the source node's red slot
+    // of direction I, then the pair the colour sums add and the total gi
+    using Raw = float2;
     template <int I>
-    __device__ __forceinline__ void load_ptr(const float *p, float &r, float &b) const {
-        r = __ldg(p);
-        b = __ldg(p + 3 * NX);
+    __device__ __forceinline__ Raw load_raw(const float *p) const {
+        return make_float2(__ldg(p), __ldg(p + 3 * NX));
+    }
+    template <int I>
+    __device__ __forceinline__ float2 decode(Raw v, float &gi) const {
+        gi = v.x + v.y;
+        return v;
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
@@ -156,9 +162,21 @@ struct CodecF16 {
     // the same through `p` = the source node's word of direction I
     template <int I>
     __device__ __forceinline__ void load_sd_ptr(const __half2 *p, float &gs, float &d) const {
-        const float2 v = __half22float2(__ldg(p));
-        gs = fmaf(Dir<I>::w, v.x, Dir<I>::w * rho0);
-        d = fmaf(-gs, v.y, copysignf(gs, v.y));
+        const float2 v = decode<I>(__ldg(p), gs);
+        d = v.y;
+    }
+    // pull in two halves: the raw word, then (sum, difference) and the total gi
+    using Raw = __half2;
+    template <int I>
+    __device__ __forceinline__ Raw load_raw(const __half2 *p) const {
+        return __ldg(p);
+    }
+    template <int I>
+    __device__ __forceinline__ float2 decode(Raw h, float &gi) const {
+        const float2 v = __half22float2(h);
+        const float gs = fmaf(Dir<I>::w, v.x, Dir<I>::w * rho0);
+        gi = gs;
+        return make_float2(gs, fmaf(-gs, v.y, copysignf(gs, v.y)));
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
@@ -349,32 +367,46 @@ __device__ __forceinline__ void moment_add(float &acc, float v) {
         acc += v;
 }
 
-// One pulled direction as the pair the colour sums add: (fr, fb), or
-// (fr + fb, fr - fb) for C::kSumDiff; `gi` is the total fr + fb.
-template <class C, int I, class Map>
-__device__ __forceinline__ float2 pull_pair(const Map &pm, const C &codec, int x, float &gi) {
-    const typename C::Elem *p = pm.template ptr<I>(codec, x);
-    float u, v;
-    if constexpr (C::kSumDiff) {
-        codec.template load_sd_ptr<I>(p, u, v);
-        gi = u;
-    } else {
-        codec.template load_ptr<I>(p, u, v);
-        gi = u + v;
-    }
-    return make_float2(u, v);
+// A node's pull in two halves: pull_issue loads the 27 raw words (54 for
+// float32) into registers; densities_of / moments_of decode and sum them.
+// Between the two a warp can do other work while the loads are in flight.
+template <class C>
+struct RawPull {
+    typename C::Raw v[kQ];
+};
+
+template <class C, class Map>
+__device__ __forceinline__ void pull_issue_map(const Map &pm, const C &codec, int x, RawPull<C> &raw) {
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        raw.v[i] = codec.template load_raw<i>(pm.template ptr<i>(codec, x));
+    });
 }
 
 // Colour densities only of interior node (x,y,z): the colour sums of
 // pull_moments below in the same order (direction index), so psi formed from
 // either is bit-identical.  Nodes whose psi is all that is needed (halo rows
 // and planes of a tile) take this.
-template <class C, class Map>
-__device__ __forceinline__ void pull_densities_from(const Map &pm, const C &codec, int x, float &rr, float &rb) {
+// The pulled pairs come from `src.get<I>(gi)`: decoded from words already in
+// registers (RawSource) or loaded and decoded on the spot (DecodedPull).
+template <class C>
+struct RawSource {
+    const C &codec;
+    const RawPull<C> &raw;
+    template <int I>
+    __device__ __forceinline__ float2 get(float &gi) const {
+        return codec.template decode<I>(raw.v[I], gi);
+    }
+};
+
+template <class Src>
+__device__ __forceinline__ void densities_from(const Src &src, float &rr, float &rb) {
+    using C = std::remove_cv_t<std::remove_reference_t<decltype(src.codec)>>;
     float2 sum = make_float2(0.f, 0.f);  // (sum fr, sum fb); C::kSumDiff: (sum fr+fb, sum fr-fb)
     static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
         float gi;
-        sum = __fadd2_rn(sum, pull_pair<C, decltype(I)::value>(pm, codec, x, gi));  // both colours in one packed add
+        sum = __fadd2_rn(sum, src.template get<i>(gi));  // both colours in one packed add
     });
     if constexpr (C::kSumDiff) {
         rr = 0.5f * (sum.x + sum.y);
@@ -392,13 +424,14 @@ __device__ __forceinline__ void pull_densities_from(const Map &pm, const C &code
 // the moments are then formed from the sums and differences of opposite
 // pairs, about 100 operations instead of one multiply-add per direction and
 // moment.
-template <class C, class Map>
-__device__ __forceinline__ NodeMoments pull_moments_from(const Map &pm, const C &codec, int x) {
+template <class Src>
+__device__ __forceinline__ NodeMoments moments_from(const Src &src) {
+    using C = std::remove_cv_t<std::remove_reference_t<decltype(src.codec)>>;
     float2 sum = make_float2(0.f, 0.f);  // (sum fr, sum fb); C::kSumDiff: (sum fr+fb, sum fr-fb)
     float gv[kQ];                        // totals fr + fb per direction
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
-        sum = __fadd2_rn(sum, pull_pair<C, i>(pm, codec, x, gv[i]));
+        sum = __fadd2_rn(sum, src.template get<i>(gv[i]));
     });
     // Moments over the 13 opposite pairs (i, i+1), i odd: d = g_i - g_opp
     // carries the first moments, s = g_i + g_opp the second.  Near equilibrium
@@ -453,17 +486,46 @@ __device__ __forceinline__ NodeMoments pull_moments_from(const Map &pm, const C 
 // Rows 2 .. NY-3 take FastPullMap, the two edge rows PullMap (ghost planes,
 // y wrap); y is uniform over a warp at every call site, so the branch is too.
 template <class C, bool kPeriodic>
+__device__ __forceinline__ void pull_issue(const Geometry &g, const C &codec, int x, int y, int z, RawPull<C> &raw) {
+    if (y >= 2 && y <= g.NY - 3)
+        pull_issue_map(FastPullMap<C>(g, codec, x, y, z), codec, x, raw);
+    else
+        pull_issue_map(PullMap<C>(g, x, y, z, kPeriodic), codec, x, raw);
+}
+// One-piece pulls: each load is decoded where it is issued, which lets the
+// compiler consume the words as they arrive (measured 2 % faster at 80
+// registers than issuing all of them first).  The arithmetic and its order
+// are the same either way, so the results are bit-identical.
+template <class C, class Map>
+struct DecodedPull {
+    const Map &pm;
+    const C &codec;
+    int x;
+    template <int I>
+    __device__ __forceinline__ float2 get(float &gi) const {
+        return codec.template decode<I>(codec.template load_raw<I>(pm.template ptr<I>(codec, x)), gi);
+    }
+};
+template <class C, class Map>
+__device__ __forceinline__ void pull_densities_map(const Map &pm, const C &codec, int x, float &rr, float &rb) {
+    densities_from(DecodedPull<C, Map>{pm, codec, x}, rr, rb);
+}
+template <class C, class Map>
+__device__ __forceinline__ NodeMoments pull_moments_map(const Map &pm, const C &codec, int x) {
+    return moments_from(DecodedPull<C, Map>{pm, codec, x});
+}
+template <class C, bool kPeriodic>
 __device__ __forceinline__ void pull_densities(const Geometry &g, const C &codec, int x, int y, int z, float &rr,
                                                float &rb) {
     if (y >= 2 && y <= g.NY - 3)
-        pull_densities_from(FastPullMap<C>(g, codec, x, y, z), codec, x, rr, rb);
+        pull_densities_map(FastPullMap<C>(g, codec, x, y, z), codec, x, rr, rb);
     else
-        pull_densities_from(PullMap<C>(g, x, y, z, kPeriodic), codec, x, rr, rb);
+        pull_densities_map(PullMap<C>(g, x, y, z, kPeriodic), codec, x, rr, rb);
 }
 template <class C, bool kPeriodic>
 __device__ __forceinline__ NodeMoments pull_moments(const Geometry &g, const C &codec, int x, int y, int z) {
-    if (y >= 2 && y <= g.NY - 3) return pull_moments_from(FastPullMap<C>(g, codec, x, y, z), codec, x);
-    return pull_moments_from(PullMap<C>(g, x, y, z, kPeriodic), codec, x);
+    if (y >= 2 && y <= g.NY - 3) return pull_moments_map(FastPullMap<C>(g, codec, x, y, z), codec, x);
+    return pull_moments_map(PullMap<C>(g, x, y, z, kPeriodic), codec, x);
 }
 
 // Relax one node and store its 54 post-collision values (lbm.cuh:184-293).
@@ -616,11 +678,110 @@ __device__ __forceinline__ void prefetch_pull_group(const Geometry &g, const C &
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
 
-// One node of a tile row in plane zp, pulled: psi into `ring_row` (all
-// columns, halo rows included), and for own rows the moments into `msm_row`,
-// the fluid-plane moments for the boundary launch, the adjoint's moment
-// record, and the radial statistics.  Warp-collective when kStats: all 32
-// lanes of a warp (one row) call it together.
+// Own-row results of a pulled node: the moments into the stage row, the
+// fluid-plane moments for the boundary launch, the adjoint's moment record.
+template <class C>
+__device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, int y, int zp, const NodeMoments &m,
+                                                   float ps, float *msm_row, int tpr) {
+    const Geometry &g = s.g;
+    float *q = msm_row + x;
+    q[kMomRR * tpr] = m.rr;
+    q[kMomRB * tpr] = m.rb;
+    q[kMomUX * tpr] = m.ux;
+    q[kMomUY * tpr] = m.uy;
+    q[kMomUZ * tpr] = m.uz;
+    q[kMomPXX * tpr] = m.pxx;
+    q[kMomPXY * tpr] = m.pxy;
+    q[kMomPYY * tpr] = m.pyy;
+    q[kMomPYZ * tpr] = m.pyz;
+    q[kMomPZZ * tpr] = m.pzz;
+    q[kMomPXZ * tpr] = m.pxz;
+    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
+        // fluid-plane moments for the boundary launch
+        float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
+        const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
+#pragma unroll
+        for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
+    }
+    if (std::is_same<C, CodecF32>::value && s.tape) {
+        // moment record of the pulled state (the adjoint sweep reads it)
+        float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
+        const size_t N = g.N;
+        const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, ps};
+#pragma unroll
+        for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
+    }
+}
+
+// One node of a tile row in plane zp, pulled in two halves.  tile_pull_issue
+// loads the node's words (at a position that is not pulled, its psi);
+// tile_pull_finish puts psi into `ring_row` (all columns, halo rows
+// included), and for own rows the moments into `msm_row`, the fluid-plane
+// moments for the boundary launch, the adjoint's moment record, and the
+// radial statistics.  tile_pull_finish is warp-collective when kStats: all
+// 32 lanes of a warp (one row) call it together.  TilePull holds the loads
+// between the two.
+template <class C>
+struct TilePull {
+    RawPull<C> raw;  // the node's pulled words, when `pull`
+    float ps;        // psi of a position that is not pulled (ghost)
+    bool pull;
+};
+
+template <class C, bool kPeriodic>
+__device__ __forceinline__ void tile_pull_issue(const DeviceState &s, const C &codec, const float *__restrict__ psi_g,
+                                                int x, int y, int zp, TilePull<C> &t) {
+    const Geometry &g = s.g;
+    t.pull = false;
+    if (x >= g.NX) return;
+    int xn = x, yn = y, zn = zp;
+    if constexpr (kPeriodic) {
+        xn = wrap_interior(x, g.NX);
+        yn = wrap_interior(y, g.NY);
+        zn = wrap_interior(zp, g.NZ);
+        t.pull = true;
+    } else {
+        t.pull = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && zp >= 1 && zp <= g.NZ - 2;
+    }
+    if (t.pull)
+        pull_issue<C, kPeriodic>(g, codec, xn, yn, zn, t.raw);
+    else
+        t.ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
+}
+
+template <class C, bool kStats, bool kPeriodic>
+__device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &codec, int x, int y, int zp,
+                                                 bool own_row, const TilePull<C> &t, float *ring_row, float *msm_row,
+                                                 int tpr) {
+    const Geometry &g = s.g;
+    const bool xin = x >= 1 && x <= g.NX - 2;
+    NodeMoments m{};
+    bool have = false;
+    if (x < g.NX) {
+        float ps;
+        if (t.pull && own_row) {  // own_row is uniform per warp: a warp covers part of one row
+            m = moments_from(RawSource<C>{codec, t.raw});
+            have = true;
+            ps = psi_of(m.rr, m.rb);
+        } else if (t.pull) {
+            float rr, rb;
+            densities_from(RawSource<C>{codec, t.raw}, rr, rb);
+            ps = psi_of(rr, rb);
+        } else {
+            ps = t.ps;
+        }
+        ring_row[x] = ps;
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
+    }
+    if constexpr (kStats) {
+        if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
+    }
+}
+
+// tile_pull_issue + tile_pull_finish in one piece, for marches with nothing
+// to overlap: the own-row / halo branch comes before the loads, so each
+// branch consumes its loads as they arrive (issuing all of them before the
+// branch keeps every word live at once and spills at 80 registers).
 template <class C, bool kStats, bool kPeriodic>
 __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, const float *__restrict__ psi_g, int x,
                                           int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr) {
@@ -652,35 +813,7 @@ __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, 
             ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
         }
         ring_row[x] = ps;
-        if (own_row && xin) {
-            float *q = msm_row + x;
-            q[kMomRR * tpr] = m.rr;
-            q[kMomRB * tpr] = m.rb;
-            q[kMomUX * tpr] = m.ux;
-            q[kMomUY * tpr] = m.uy;
-            q[kMomUZ * tpr] = m.uz;
-            q[kMomPXX * tpr] = m.pxx;
-            q[kMomPXY * tpr] = m.pxy;
-            q[kMomPYY * tpr] = m.pyy;
-            q[kMomPYZ * tpr] = m.pyz;
-            q[kMomPZZ * tpr] = m.pzz;
-            q[kMomPXZ * tpr] = m.pxz;
-            if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
-                // fluid-plane moments for the boundary launch
-                float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
-                const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
-#pragma unroll
-                for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
-            }
-            if (std::is_same<C, CodecF32>::value && s.tape) {
-                // moment record of the pulled state (the adjoint sweep reads it)
-                float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
-                const size_t N = g.N;
-                const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, ps};
-#pragma unroll
-                for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
-            }
-        }
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
     }
     if constexpr (kStats) {
         if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
@@ -866,6 +999,10 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_PIPE_MIN_BLOCKS) k_fused_pi
     const bool xin = x >= 1 && x <= g.NX - 2;
     const bool down = T.alternate && (blockIdx.y & 1);
     auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
+    // Float16 words (27 registers a node) stay in flight across the relaxation
+    // of another row: measured +4 % on 128x256x128.  Float32 (54 registers)
+    // measured 1 % slower that way and pulls then relaxes.
+    constexpr bool kOverlap = std::is_same<C, CodecF16>::value;
     for (int k = 0; k <= lz + 2; ++k) {
         const bool do_pull = k <= lz + 1;
         const int c = k - 2;  // march index of the plane relaxed in this iteration
@@ -883,12 +1020,24 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_PIPE_MIN_BLOCKS) k_fused_pi
         // 1+lr, 1+lr+rpt, ... (<= ty), interleaved so that a warp has loads of
         // one row in flight while it relaxes another
         for (int r = lr; r < ty + 2; r += rpt) {
-            if (do_pull)
-                tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
-                                                ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
+            const bool own = own_plane && r >= 1 && r <= ty;
             const int rc = r + 1;
-            if (do_relax && rc <= ty && xin)
-                tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+            if constexpr (kOverlap) {
+                // the loads of row r are in flight while this warp relaxes row r+1
+                TilePull<C> tp;
+                if (do_pull) tile_pull_issue<C, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, tp);
+                if (do_relax && rc <= ty && xin)
+                    tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+                if (do_pull)
+                    tile_pull_finish<C, kStats, kPeriodic>(s, codec, x, y0 - 1 + r, zp, own, tp, ringp + r * tpr,
+                                                           msmp + (r - 1) * kMomCount * tpr, tpr);
+            } else {
+                if (do_pull)
+                    tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own, ringp + r * tpr,
+                                                    msmp + (r - 1) * kMomCount * tpr, tpr);
+                if (do_relax && rc <= ty && xin)
+                    tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+            }
         }
         __syncthreads();
     }
@@ -2084,11 +2233,11 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     const int per_row = t.tpr * 4;
     const int rpt = kFusedThreads / t.tpr;
     if (const char *v = std::getenv("MCG_FUSED_SMEM_KB")) max_smem = std::atoi(v) * 1024;  // tuning sweeps
-    // software-pipelined march for float32 rows of up to 128 columns (4-row
-    // tiles at two CTAs per SM; measured +5 % on 128x256x128).  Float16 is
-    // issue-bound and rows of 256 columns need 2-row tiles: the
-    // block-synchronous march measured faster there.
-    t.pipe = g.storage == kStoreF32 && t.tpr <= 128;
+    // software-pipelined march for rows of up to 128 columns (4-row tiles at
+    // two CTAs per SM; measured on 128x256x128: +5 % float32, and +2 % float16
+    // with its loads in flight across the relaxation).  Rows of 256 columns
+    // need 2-row tiles: the block-synchronous march measured faster there.
+    t.pipe = t.tpr <= 128;
     if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v) != 0;  // tuning sweeps
     if (t.pipe) max_smem = std::max(max_smem, 112 * 1024);  // 4 ring + 3 stage planes: two CTAs per SM
     // rows per tile: at least one round of rows in parallel, 4 by default
