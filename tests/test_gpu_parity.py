@@ -227,3 +227,32 @@ def test_fixed_row_length_kernels_equal_runtime_geometry(monkeypatch, storage, n
     np.testing.assert_array_equal(pa[1], pb[1])
     for k in fa:
         np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("name,shape", [("jet_24x40x24", (40, 32, 36)), ("bubble_64", (72, 20, 34))])
+def test_pipelined_march_equals_block_synchronous_march(monkeypatch, storage, name, shape):
+    """k_fused_pipe (one barrier per plane; float16 with its loads in flight
+    across another row's relaxation) and k_fused (two barriers per plane) do
+    the same arithmetic in the same order: equal populations and fields, bit
+    for bit, on row lengths other than 128 (64 and 96 threads per row, idle
+    lanes included) and 16-plane chunks."""
+    NX, NY, NZ = shape
+    case = get_case(name, NX=NX, NY=NY, NZ=NZ, storage=storage, NSTATS_START_STEP=0)
+    state = initial_state(case, noise=1e-3 if case["boundary"] != "jet" else 0.0, seed=17)
+    monkeypatch.setenv("MCG_FUSED_LZ", "16")
+    out = []
+    for pipe in ("1", "0"):
+        monkeypatch.setenv("MCG_FUSED_PIPE", pipe)
+        with _solver_from_state(case, state) as S:
+            t = S.tiling()
+            assert t["pipelined"] == int(pipe) and t["fixed_row_length"] == 0
+            S.step(25)
+            out.append((S.get_populations(), S.get_fields(), S.get_radial() if case["boundary"] == "jet" else None))
+    (pa, fa, ra), (pb, fb, rb) = out
+    np.testing.assert_array_equal(pa[0], pb[0])
+    np.testing.assert_array_equal(pa[1], pb[1])
+    for k in fa:
+        np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
+    if case["boundary"] == "jet":
+        _radial_close(ra, rb, atol=1e-9)
