@@ -238,7 +238,7 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
     if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
     const mcg::Geometry &g = h->s.g;
     const size_t N = g.N;
-    const size_t pop_bytes = size_t(g.slots) * N * sizeof(float);
+    const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
     const size_t record_floats = size_t(mcg::kTapePlanes) * N;
     const bool tape_mode = snapshots > nsteps;
     const int free_slots = tape_mode ? 0 : snapshots - 1;
@@ -354,7 +354,7 @@ mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, i
     if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
     const mcg::Geometry &g = h->s.g;
     const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
-    const size_t pop_bytes = size_t(g.slots) * N * sizeof(float);
+    const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
     const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
     const int nb = mcg::kInletBesselMax;
 

@@ -324,7 +324,7 @@ mcg_status mcg_create(const mcg_params *p, mcg_handle **out) {
     g.sz = p->NX * p->NY;
     g.boundary = p->boundary;
     g.storage = p->storage;
-    g.slots = p->storage == MCG_STORAGE_F16 ? mcg::kQ : 2 * mcg::kQ;
+    g.slots = mcg::kQ;  // one element (both colours) per direction: float2 or half2
     fill_physics(h);
     compute_ncols(h);
     const size_t N = g.N;

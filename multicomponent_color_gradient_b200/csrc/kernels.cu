@@ -43,40 +43,41 @@ constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------ storage codecs
 
+// Float32 element per (direction, node): the pair (fr, fb), so a pull or a
+// store of both colours is one 8-byte access.
 struct CodecF32 {
-    using Elem = float;
-    static constexpr int kGroupSlots = 6;
+    using Elem = float2;
+    static constexpr int kGroupSlots = 3;
     static constexpr bool kSumDiff = false;  // pulls form sum fr and sum fb (reference order)
-    const float *__restrict__ rd;
-    float *__restrict__ wr;
+    const float2 *__restrict__ rd;
+    float2 *__restrict__ wr;
     int NX;
     // store through `wrow` = the node's row in the written buffer, offset by x
     template <int I>
-    __device__ __forceinline__ void store_row(float *wrow, float r, float b) const {
-        wrow[slot_f32(I, 0) * NX] = r;
-        wrow[slot_f32(I, 1) * NX] = b;
+    __device__ __forceinline__ void store_row(float2 *wrow, float r, float b) const {
+        wrow[slot_pair(I) * NX] = make_float2(r, b);
     }
     // bulk node: fr_i = aR w_i P_i, fb_i = aB w_i P_i (lbm.cuh:216-247)
-    __device__ __forceinline__ void store_bulk(float *wrow, float aR, float aB, const float (&P)[kQ]) const {
+    __device__ __forceinline__ void store_bulk(float2 *wrow, float aR, float aB, const float (&P)[kQ]) const {
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            // both colours in one packed multiply
-            const float2 f = __fmul2_rn(make_float2(aR * Dir<i>::w, aB * Dir<i>::w), make_float2(P[i], P[i]));
-            store_row<i>(wrow, f.x, f.y);
+            // both colours in one packed multiply and one store
+            wrow[slot_pair(i) * NX] = __fmul2_rn(make_float2(aR * Dir<i>::w, aB * Dir<i>::w), make_float2(P[i], P[i]));
         });
     }
     // pull: `grow` = offset of the source row's group segment
     template <int I>
     __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
-        r = __ldg(rd + grow + size_t(0 * 3 + dir_cx(I) + 1) * NX + xs);
-        b = __ldg(rd + grow + size_t(1 * 3 + dir_cx(I) + 1) * NX + xs);
+        const float2 v = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
+        r = v.x;
+        b = v.y;
     }
-    // pull in two halves: the raw words at `p` = the source node's red slot
-    // of direction I, then the pair the colour sums add and the total gi
+    // pull in two halves: the raw pair at `p` = the source node's element of
+    // direction I, then the pair the colour sums add and the total gi
     using Raw = float2;
     template <int I>
-    __device__ __forceinline__ Raw load_raw(const float *p) const {
-        return make_float2(__ldg(p), __ldg(p + 3 * NX));
+    __device__ __forceinline__ Raw load_raw(const float2 *p) const {
+        return __ldg(p);
     }
     template <int I>
     __device__ __forceinline__ float2 decode(Raw v, float &gi) const {
@@ -85,22 +86,32 @@ struct CodecF32 {
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
-        wr[row + size_t(slot_f32(I, 0)) * NX + x] = r;
-        wr[row + size_t(slot_f32(I, 1)) * NX + x] = b;
+        wr[row + size_t(slot_pair(I)) * NX + x] = make_float2(r, b);
     }
     __device__ __forceinline__ static void store_to(void *buf, const Geometry &g, int i, int x, int y, int z, float r,
                                                     float b, float) {
-        float *p = static_cast<float *>(buf);
-        p[pop_index(g, slot_f32(i, 0), x, y, z)] = r;
-        p[pop_index(g, slot_f32(i, 1), x, y, z)] = b;
+        static_cast<float2 *>(buf)[pop_index(g, slot_pair(i), x, y, z)] = make_float2(r, b);
     }
     __device__ __forceinline__ static void load_from(const void *buf, const Geometry &g, int i, int x, int y, int z,
                                                      float &r, float &b, float) {
-        const float *p = static_cast<const float *>(buf);
-        r = p[pop_index(g, slot_f32(i, 0), x, y, z)];
-        b = p[pop_index(g, slot_f32(i, 1), x, y, z)];
+        const float2 v = static_cast<const float2 *>(buf)[pop_index(g, slot_pair(i), x, y, z)];
+        r = v.x;
+        b = v.y;
     }
 };
+
+// Layout of the adjoint's lambda arrays: separate colour rows, 6 x-rows per
+// pull-source segment (slot_f32), 54 float x-rows per lattice row.  PullMap
+// over it gives lambda's source offsets; lam_geometry gives its row stride.
+struct LamLayout {
+    using Elem = float;
+    static constexpr int kGroupSlots = 6;
+};
+__host__ __device__ __forceinline__ Geometry lam_geometry(const Geometry &g) {
+    Geometry l = g;
+    l.slots = 2 * kQ;
+    return l;
+}
 
 // F16 word per (direction, node): x = g/w_i - rho0 (total offset by the rest
 // equilibrium and scaled by 1/w_i), y = q, the minority-colour fraction
@@ -133,7 +144,7 @@ struct CodecF16 {
     float rho0;
     template <int I>
     __device__ __forceinline__ void store_row(__half2 *wrow, float r, float b) const {
-        wrow[slot_f16(I) * NX] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
+        wrow[slot_pair(I) * NX] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
     }
     // bulk node: every direction splits its total g_i = w_i P_i in the same
     // proportion aR : aB, so the word is (P_i - rho0, q) with one signed
@@ -144,7 +155,7 @@ struct CodecF16 {
         const float q = copysignf(fmaxf(2.0f * fminf(aR, aB), 0.0f), aR - aB);
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            wrow[slot_f16(i) * NX] = __floats2half2_rn(P[i] - rho0, q);
+            wrow[slot_pair(i) * NX] = __floats2half2_rn(P[i] - rho0, q);
         });
     }
     template <int I>
@@ -180,15 +191,15 @@ struct CodecF16 {
     }
     template <int I>
     __device__ __forceinline__ void store(size_t row, int x, float r, float b) const {
-        wr[row + size_t(slot_f16(I)) * NX + x] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
+        wr[row + size_t(slot_pair(I)) * NX + x] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
     }
     __device__ __forceinline__ static void store_to(void *buf, const Geometry &g, int i, int x, int y, int z, float r,
                                                     float b, float rho0) {
-        static_cast<__half2 *>(buf)[pop_index(g, slot_f16(i), x, y, z)] = f16_encode(r, b, 1.0f / dir_w(i), rho0);
+        static_cast<__half2 *>(buf)[pop_index(g, slot_pair(i), x, y, z)] = f16_encode(r, b, 1.0f / dir_w(i), rho0);
     }
     __device__ __forceinline__ static void load_from(const void *buf, const Geometry &g, int i, int x, int y, int z,
                                                      float &r, float &b, float rho0) {
-        f16_decode(static_cast<const __half2 *>(buf)[pop_index(g, slot_f16(i), x, y, z)], dir_w(i), rho0, r, b);
+        f16_decode(static_cast<const __half2 *>(buf)[pop_index(g, slot_pair(i), x, y, z)], dir_w(i), rho0, r, b);
     }
 };
 
@@ -196,7 +207,7 @@ template <class C>
 __host__ __device__ C make_codec(const DeviceState &s, int cur);
 template <>
 __host__ __device__ CodecF32 make_codec<CodecF32>(const DeviceState &s, int cur) {
-    return CodecF32{static_cast<const float *>(s.pops[cur]), static_cast<float *>(s.pops[cur ^ 1]), s.g.NX};
+    return CodecF32{static_cast<const float2 *>(s.pops[cur]), static_cast<float2 *>(s.pops[cur ^ 1]), s.g.NX};
 }
 template <>
 __host__ __device__ CodecF16 make_codec<CodecF16>(const DeviceState &s, int cur) {
@@ -1593,7 +1604,7 @@ __device__ __forceinline__ double block_sum_any(double v, double *sh, int nthrea
 __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s, const float *__restrict__ M,
                                                            const float *__restrict__ target, float *lam, double *J) {
     __shared__ double sh[kBX * kBY / 32];
-    const Geometry &g = s.g;
+    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -1609,7 +1620,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
         const float lpsi = 2.0f * d;
         const float inv2 = 1.0f / (rho * rho);
         const float lrr = lpsi * 2.0f * rb * inv2, lrb = -lpsi * 2.0f * rr * inv2;
-        const PullMap<CodecF32> pm(g, x, y, z, true);
+        const PullMap<LamLayout> pm(g, x, y, z, true);
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
             size_t grow;
@@ -1641,7 +1652,7 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
                                                              const float *lam, float *lmom, float *lf, double *acc,
                                                              AdjObjective obj) {
     __shared__ double sh[kBX * kBY / 32];
-    const Geometry &g = s.g;
+    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
     const Physics &ph = s.ph;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
@@ -1863,7 +1874,7 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
 template <bool kPeriodic>
 __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *__restrict__ M,
                                                           const float *lmom, const float *lf, float *lam_out) {
-    const Geometry &g = s.g;
+    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -1910,7 +1921,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     const float invr = 1.0f / rho;
     const float ljx = lux * invr, ljy = luy * invr, ljz = luz * invr;
     lrho -= (lux * ux + luy * uy + luz * uz) * invr;
-    const PullMap<CodecF32> pm(g, x, y, z, kPeriodic);
+    const PullMap<LamLayout> pm(g, x, y, z, kPeriodic);
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         using D = Dir<i>;
@@ -1981,7 +1992,7 @@ __global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64
                                                       const float *__restrict__ lf, float *lmom,
                                                       const float *__restrict__ LB_in, float *LB_out,
                                                       const float *__restrict__ bessel, int nb, double *dJdc) {
-    const Geometry &g = s.g;
+    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
     const Physics &ph = s.ph;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.y * blockDim.y + threadIdx.y;
@@ -2181,7 +2192,7 @@ __global__ void __launch_bounds__(256) k_copy_outlet_state(const DeviceState s, 
 // the forward step pulls populations.
 __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, const float *__restrict__ M,
                                                           const float *lam0, float *du0) {
-    const Geometry &g = s.g;
+    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -2196,7 +2207,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, 
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const EqTerms e = make_eq(ux, uy, uz);
-    const PullMap<CodecF32> pm(g, x, y, z, true);
+    const PullMap<LamLayout> pm(g, x, y, z, true);
     float gx = 0.f, gy = 0.f, gz = 0.f, gq = 0.f;
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;

@@ -2,16 +2,19 @@
 //
 // HBM layout (node index id = x + NX*(y + NY*z) for the per-node fields):
 //   pops[2]   two population buffers (ping-pong), row-blocked: row (y,z) holds
-//             `slots` x-rows of NX values, grouped by pull source (lattice.cuh
-//             slot_f32 / slot_f16); element (slot, x, y, z) is at
-//             ((z*NY + y)*slots + slot)*NX + x.
+//             `slots` = 27 x-rows of NX elements, grouped by pull source
+//             (lattice.cuh slot_pair); element (slot, x, y, z) is at
+//             ((z*NY + y)*27 + slot)*NX + x.  One element carries both colours
+//             of a direction, so a pull or a store is one 8- or 4-byte access.
 //             A buffer holds, at node s and direction i, the value that streams
 //             OUT of s along c_i (post-collision, pull layout): node x reads
 //             f_i(x) from x - c_i.  The y ghost planes hold what the boundary
 //             delivers into the first/last fluid plane.
-//               F32: float,   slots = 54 (27 directions x 2 colours)
-//               F16: __half2, slots = 27 ((total offset by w_i*rho0)/w_i,
-//                                         signed minority-colour fraction)
+//               F32: float2 (fr, fb)
+//               F16: __half2 ((total offset by w_i*rho0)/w_i, signed
+//                              minority-colour fraction)
+//             The adjoint's lambda arrays keep separate colour rows: 54
+//             float x-rows per row (slot_f32), indexed through lam_geometry.
 //   mom       11 float planes [11][N]: rr, rb, ux, uy, uz, Pixx, Pixy, Piyy,
 //             Piyz, Pizz, Pixz - the reference's LbmDevice fields
 //             (memory.cuh:11-25), ghost nodes included.  The fused step does
