@@ -981,12 +981,17 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
 // a CTA drift apart, and the memory-bound pull of one warp overlaps the
 // ALU-bound relaxation of another.
 constexpr int kPipeRing = 4, kPipeStage = 3;
-#ifndef MCG_PIPE_MIN_BLOCKS
-#define MCG_PIPE_MIN_BLOCKS 2
-#endif
+// CTAs per SM the pipelined kernel's register budget is sized for: float32
+// (3-row tiles, 3 CTAs, 80 registers) measured faster than 2 CTAs at 128
+// registers; float16 keeps 2 (its words in flight across the relaxation need
+// the registers).
+template <class C>
+struct PipeBlocks {
+    static constexpr int value = std::is_same<C, CodecF16>::value ? 2 : 3;
+};
 
 template <class C, bool kStats, bool kPeriodic, int kNX>
-__global__ void __launch_bounds__(kFusedThreads, MCG_PIPE_MIN_BLOCKS) k_fused_pipe(const DeviceState s_arg,
+__global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_pipe(const DeviceState s_arg,
                                                                                   const FusedTiling T, int cur,
                                                                                   int64_t step) {
     extern __shared__ float sm[];
@@ -2255,6 +2260,9 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     // (measured best on 128x256x128), fewer if shared memory
     // (3*(ty+2) + 2*11*ty) * tpr * 4 bytes does not fit
     int ty = std::max(4, rpt);
+    // the float32 pipelined march runs 3 CTAs per SM (PipeBlocks) on one round
+    // of rows (2 rows for 128 columns; measured +1.5 % over 4-row tiles at 2 CTAs)
+    if (t.pipe && g.storage == kStoreF32) ty = std::max(2, rpt);
     if (const char *v = std::getenv("MCG_FUSED_TY")) ty = std::max(1, std::atoi(v));  // tuning sweeps
     auto smem_of = [&](int h) {
         return (t.pipe ? kPipeRing * (h + 2) + kPipeStage * kMomCount * h : 3 * (h + 2) + 2 * kMomCount * h) * per_row;
