@@ -100,19 +100,6 @@ struct CodecF32 {
     }
 };
 
-// Layout of the adjoint's lambda arrays: separate colour rows, 6 x-rows per
-// pull-source segment (slot_f32), 54 float x-rows per lattice row.  PullMap
-// over it gives lambda's source offsets; lam_geometry gives its row stride.
-struct LamLayout {
-    using Elem = float;
-    static constexpr int kGroupSlots = 6;
-};
-__host__ __device__ __forceinline__ Geometry lam_geometry(const Geometry &g) {
-    Geometry l = g;
-    l.slots = 2 * kQ;
-    return l;
-}
-
 // F16 word per (direction, node): x = g/w_i - rho0 (total offset by the rest
 // equilibrium and scaled by 1/w_i), y = q, the minority-colour fraction
 // 2 min(fr,fb)/g carrying the sign of fr-fb.  Pure nodes store q = +-0
@@ -1609,7 +1596,7 @@ __device__ __forceinline__ double block_sum_any(double v, double *sh, int nthrea
 __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s, const float *__restrict__ M,
                                                            const float *__restrict__ target, float *lam, double *J) {
     __shared__ double sh[kBX * kBY / 32];
-    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
+    const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -1625,14 +1612,13 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
         const float lpsi = 2.0f * d;
         const float inv2 = 1.0f / (rho * rho);
         const float lrr = lpsi * 2.0f * rb * inv2, lrb = -lpsi * 2.0f * rr * inv2;
-        const PullMap<LamLayout> pm(g, x, y, z, true);
+        const PullMap<CodecF32> pm(g, x, y, z, true);
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
             size_t grow;
             int xs;
             pm.template src<i>(x, grow, xs);
-            lam[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrr;
-            lam[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrb;
+            reinterpret_cast<float2 *>(lam)[grow + size_t(dir_cx(i) + 1) * g.NX + xs] = make_float2(lrr, lrb);
         });
     }
     const double r = block_sum_any(jloc, sh, kBX * kBY);
@@ -1657,7 +1643,7 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
                                                              const float *lam, float *lmom, float *lf, double *acc,
                                                              AdjObjective obj) {
     __shared__ double sh[kBX * kBY / 32];
-    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
+    const Geometry &g = s.g;
     const Physics &ph = s.ph;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
@@ -1714,9 +1700,13 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         float sAx = 0.f, sAy = 0.f, sAz = 0.f, sB = 0.f, sDx = 0.f, sDy = 0.f, sDz = 0.f, sE = 0.f, sBB = 0.f,
               l_Ah = 0.f;
         const size_t row = pop_row(g, y, z);
-        auto lam_at = [&](int slot) { return lam[row + size_t(slot) * size_t(g.NX) + size_t(x)]; };
+        // (lambda_r, lambda_b) of a direction: one float2, as the populations
+        auto lam_at = [&](int slot) {
+            return reinterpret_cast<const float2 *>(lam)[row + size_t(slot) * size_t(g.NX) + size_t(x)];
+        };
         {  // rest direction: even only
-            const float lr = lam_at(slot_f32(0, 0)), lb = lam_at(slot_f32(0, 1));
+            const float2 l0 = lam_at(slot_pair(0));
+            const float lr = l0.x, lb = l0.y;
             const float lg = aR * lr + aB * lb, ld = lr - lb;
             const float w = Dir<0>::w;
             const float E = 1.0f - usq * kInv2Cs2;
@@ -1740,8 +1730,8 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         static_for<(kQ - 1) / 2>([&](auto P) {
             constexpr int i = 2 * decltype(P)::value + 1;
             using D = Dir<i>;
-            const float lri = lam_at(slot_f32(i, 0)), lbi = lam_at(slot_f32(i, 1));
-            const float lro = lam_at(slot_f32(i + 1, 0)), lbo = lam_at(slot_f32(i + 1, 1));
+            const float2 li = lam_at(slot_pair(i)), lo = lam_at(slot_pair(i + 1));
+            const float lri = li.x, lbi = li.y, lro = lo.x, lbo = lo.y;
             const float lgi = aR * lri + aB * lbi, lgo = aR * lro + aB * lbo;
             const float ldi = lri - lbi, ldo = lro - lbo;
             const float gs = lgi + lgo, gd = lgi - lgo, ds = ldi + ldo, dd = ldi - ldo;
@@ -1879,7 +1869,7 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
 template <bool kPeriodic>
 __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *__restrict__ M,
                                                           const float *lmom, const float *lf, float *lam_out) {
-    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
+    const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -1926,7 +1916,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     const float invr = 1.0f / rho;
     const float ljx = lux * invr, ljy = luy * invr, ljz = luz * invr;
     lrho -= (lux * ux + luy * uy + luz * uz) * invr;
-    const PullMap<LamLayout> pm(g, x, y, z, kPeriodic);
+    const PullMap<CodecF32> pm(g, x, y, z, kPeriodic);
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
         using D = Dir<i>;
@@ -1941,8 +1931,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
         size_t grow;
         int xs;
         pm.template src<i>(x, grow, xs);
-        lam_out[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrr + lgi;
-        lam_out[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs] = lrb + lgi;
+        reinterpret_cast<float2 *>(lam_out)[grow + size_t(dir_cx(i) + 1) * g.NX + xs] = make_float2(lrr + lgi, lrb + lgi);
     });
 }
 
@@ -1997,7 +1986,7 @@ __global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64
                                                       const float *__restrict__ lf, float *lmom,
                                                       const float *__restrict__ LB_in, float *LB_out,
                                                       const float *__restrict__ bessel, int nb, double *dJdc) {
-    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
+    const Geometry &g = s.g;
     const Physics &ph = s.ph;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.y * blockDim.y + threadIdx.y;
@@ -2036,8 +2025,8 @@ __global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64
             using D = Dir<i>;
             if constexpr (D::cy == -1) {
                 if (!pulled(x + D::cx, z + D::cz)) return;
-                const float lr = lam[pop_index(g, slot_f32(i, 0), x, g.NY - 1, z)];
-                const float lb = lam[pop_index(g, slot_f32(i, 1), x, g.NY - 1, z)];
+                const float2 l = reinterpret_cast<const float2 *>(lam)[pop_index(g, slot_pair(i), x, g.NY - 1, z)];
+                const float lr = l.x, lb = l.y;
                 const float fe = feq<i>(rho, e), fn = fneq<i>(nF);
                 const float gi = fe + oms * fn;
                 const float lg = aR * lr + aB * lb;
@@ -2130,7 +2119,7 @@ __global__ void __launch_bounds__(256) k_adj_boundary(const DeviceState s, int64
                 using D = Dir<i>;
                 if constexpr (D::cy == 1) {
                     if (!pulled(x + D::cx, z + D::cz)) return;
-                    const float lg = lam[pop_index(g, slot_f32(i, 1), x, 0, z)];  // red = 0 * g
+                    const float lg = reinterpret_cast<const float2 *>(lam)[pop_index(g, slot_pair(i), x, 0, z)].y;  // red = 0 * g
                     // d feq_i / d uy at u = (0, U, 0): w rho (c_y P - U Q), c.u = U
                     const float P = kInvCs2 + U * (2.0f * kInv2Cs4) + (U * U) * (3.0f * kInv6Cs6) - (U * U) * kInv2Cs4;
                     const float Q = kInvCs2 + U * (2.0f * kInv2Cs4);
@@ -2197,7 +2186,7 @@ __global__ void __launch_bounds__(256) k_copy_outlet_state(const DeviceState s, 
 // the forward step pulls populations.
 __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, const float *__restrict__ M,
                                                           const float *lam0, float *du0) {
-    const Geometry g = lam_geometry(s.g);  // lambda's layout (54 float x-rows per row)
+    const Geometry &g = s.g;
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
@@ -2212,7 +2201,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, 
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const EqTerms e = make_eq(ux, uy, uz);
-    const PullMap<LamLayout> pm(g, x, y, z, true);
+    const PullMap<CodecF32> pm(g, x, y, z, true);
     float gx = 0.f, gy = 0.f, gz = 0.f, gq = 0.f;
     static_for<kQ>([&](auto I) {
         constexpr int i = decltype(I)::value;
@@ -2220,8 +2209,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_initial(const DeviceState s, 
         size_t grow;
         int xs;
         pm.template src<i>(x, grow, xs);
-        const float lr = lam0[grow + size_t(0 * 3 + dir_cx(i) + 1) * g.NX + xs];
-        const float lb = lam0[grow + size_t(1 * 3 + dir_cx(i) + 1) * g.NX + xs];
+        const float2 l = reinterpret_cast<const float2 *>(lam0)[grow + size_t(dir_cx(i) + 1) * g.NX + xs];
+        const float lr = l.x, lb = l.y;
         float cu = 0.f;
         if constexpr (D::cx != 0) cu += D::fx * ux;
         if constexpr (D::cy != 0) cu += D::fy * uy;

@@ -13,8 +13,8 @@
 //               F32: float2 (fr, fb)
 //               F16: __half2 ((total offset by w_i*rho0)/w_i, signed
 //                              minority-colour fraction)
-//             The adjoint's lambda arrays keep separate colour rows: 54
-//             float x-rows per row (slot_f32), indexed through lam_geometry.
+//             The adjoint's lambda arrays have the float32 layout: one
+//             float2 (lambda_r, lambda_b) per direction and node.
 //   mom       11 float planes [11][N]: rr, rb, ux, uy, uz, Pixx, Pixy, Piyy,
 //             Piyz, Pizz, Pixz - the reference's LbmDevice fields
 //             (memory.cuh:11-25), ghost nodes included.  The fused step does

@@ -87,13 +87,11 @@ __host__ __device__ constexpr int dir_opp(int i) { return i == 0 ? 0 : ((i & 1) 
 // Row-blocked population layout.  All populations of one lattice row (y,z)
 // are contiguous; inside a row they are grouped by the row they are pulled
 // from: group g = (cy+1)*3 + (cz+1), then cx.  One element holds both colours
-// of a direction (a float2 (fr, fb), or a float16 pair), so a pulled row is 9
-// contiguous segments of 3 x-rows: slot_pair.  slot_f32 is the layout of
-// separate colour rows (group, colour, cx: 6 x-rows per segment) that the
-// adjoint's lambda arrays keep.
+// of a direction (a float2 (fr, fb), or a float16 pair; the adjoint's lambda
+// pairs (lambda_r, lambda_b) the same way), so a pulled row is 9 contiguous
+// segments of 3 x-rows.
 __host__ __device__ constexpr int dir_group(int i) { return (dir_cy(i) + 1) * 3 + (dir_cz(i) + 1); }
 __host__ __device__ constexpr int slot_pair(int i) { return dir_group(i) * 3 + (dir_cx(i) + 1); }
-__host__ __device__ constexpr int slot_f32(int i, int colour) { return dir_group(i) * 6 + colour * 3 + (dir_cx(i) + 1); }
 
 template <int... Is, class F>
 __device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, Is...>) {
