@@ -278,6 +278,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost measurement")
     ap.add_argument("--adjoint-steps", type=int, default=100)
+    ap.add_argument("--jet-adjoint-steps", type=int, default=400, help="steps of the jet-adjoint cost measurement")
+    ap.add_argument("--jet-adjoint-segment", type=int, default=100, help="checkpoint segment of the jet adjoint")
     ap.add_argument("--shape", default=None,
                     help="NXxNYxNZ override of the case grid (smaller profiling captures); not a bench line")
     args = ap.parse_args()
@@ -384,7 +386,7 @@ def main():
         except Exception as exc:
             adjoint = {"value": None, "error": str(exc)[:200]}
         try:
-            jet_adjoint = jet_adjoint_cost(400, 100)
+            jet_adjoint = jet_adjoint_cost(args.jet_adjoint_steps, args.jet_adjoint_segment)
         except Exception as exc:
             jet_adjoint = {"value": None, "error": str(exc)[:200]}
 
