@@ -365,8 +365,8 @@ __device__ __forceinline__ void moment_add(float &acc, float v) {
         acc += v;
 }
 
-// A node's pull in two halves: pull_issue loads the 27 raw words (54 for
-// float32) into registers; densities_of / moments_of decode and sum them.
+// A node's pull in two halves: pull_issue loads the 27 raw elements (float2
+// or half2) into registers; densities_of / moments_of decode and sum them.
 // Between the two a warp can do other work while the loads are in flight.
 template <class C>
 struct RawPull {

@@ -47,7 +47,7 @@ struct Geometry {
     int sy, sz;  // strides of y and z in the per-node fields: NX, NX*NY
     int boundary;
     int storage;
-    int slots;   // x-rows per lattice row in the population buffers (54 or 27)
+    int slots;   // x-rows per lattice row in the population buffers: 27 (one element per direction)
 };
 
 __host__ __device__ __forceinline__ size_t pop_row(const Geometry &g, int y, int z) {
