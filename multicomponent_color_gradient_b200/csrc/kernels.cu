@@ -366,7 +366,7 @@ __device__ __forceinline__ void moment_add(float &acc, float v) {
 }
 
 // A node's pull in two halves: pull_issue loads the 27 raw elements (float2
-// or half2) into registers; densities_of / moments_of decode and sum them.
+// or half2) into registers; densities_from / moments_from decode and sum them.
 // Between the two a warp can do other work while the loads are in flight.
 template <class C>
 struct RawPull {
@@ -1003,8 +1003,9 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     const bool down = T.alternate && (blockIdx.y & 1);
     auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
     // Float16 words (27 registers a node) stay in flight across the relaxation
-    // of another row: measured +4 % on 128x256x128.  Float32 (54 registers)
-    // measured 1 % slower that way and pulls then relaxes.
+    // of another row: measured +4 % on 128x256x128.  Float32 (27 float2, 54
+    // registers) pulls then relaxes: its 3-CTA, 80-register default is faster
+    // than the overlap, which spills there.
     constexpr bool kOverlap = std::is_same<C, CodecF16>::value;
     for (int k = 0; k <= lz + 2; ++k) {
         const bool do_pull = k <= lz + 1;
