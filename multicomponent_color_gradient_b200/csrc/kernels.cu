@@ -49,6 +49,9 @@ struct CodecF32 {
     using Elem = float2;
     static constexpr int kGroupSlots = 3;
     static constexpr bool kSumDiff = false;  // pulls form sum fr and sum fb (reference order)
+    // store_bulk takes P_i itself (collision_poly without a shift)
+    static constexpr bool kShiftPoly = false;
+    __device__ __forceinline__ float poly_shift() const { return 0.0f; }
     const float2 *__restrict__ rd;
     float2 *__restrict__ wr;
     int NX;
@@ -125,6 +128,9 @@ struct CodecF16 {
     using Elem = __half2;
     static constexpr int kGroupSlots = 3;
     static constexpr bool kSumDiff = true;  // pulls form sum (fr+fb) and sum (fr-fb)
+    // store_bulk takes P_i - rho0, formed by collision_poly's constant term
+    static constexpr bool kShiftPoly = true;
+    __device__ __forceinline__ float poly_shift() const { return rho0; }
     const __half2 *__restrict__ rd;
     __half2 *__restrict__ wr;
     int NX;
@@ -134,15 +140,16 @@ struct CodecF16 {
         wrow[slot_pair(I) * NX] = f16_encode(r, b, 1.0f / Dir<I>::w, rho0);
     }
     // bulk node: every direction splits its total g_i = w_i P_i in the same
-    // proportion aR : aB, so the word is (P_i - rho0, q) with one signed
+    // proportion aR : aB, so the word is (P_i - rho0, q) (Ps = P - rho0 from
+    // collision_poly) with one signed
     // minority fraction q = 2 min(aR, aB) for the node - the value f16_encode
     // forms from fr_i, fb_i up to float rounding, and exactly +-0 at a pure
     // node (aB or aR is exactly 0 there).
-    __device__ __forceinline__ void store_bulk(__half2 *wrow, float aR, float aB, const float (&P)[kQ]) const {
+    __device__ __forceinline__ void store_bulk(__half2 *wrow, float aR, float aB, const float (&Ps)[kQ]) const {
         const float q = copysignf(fmaxf(2.0f * fminf(aR, aB), 0.0f), aR - aB);
         static_for<kQ>([&](auto I) {
             constexpr int i = decltype(I)::value;
-            wrow[slot_pair(i) * NX] = __floats2half2_rn(P[i] - rho0, q);
+            wrow[slot_pair(i) * NX] = __floats2half2_rn(Ps[i], q);
         });
     }
     template <int I>
@@ -543,8 +550,15 @@ __device__ __forceinline__ void collide_node(const Geometry &g, const Physics &p
     const float aR = rr * invrT, aB = rb * invrT;
     const float oms = 1.0f - omega_at(ph, y);
     const float Iind = 4.0f * rr * rb * invrT * invrT;
-    float P[kQ];
-    collision_poly(rT, m.ux, m.uy, m.uz, n, oms, P);
+    float P[kQ];  // P_i - shift, shift = 0 (float32) or rho0 (float16)
+    const float shift = codec.poly_shift();
+    collision_poly(rT, m.ux, m.uy, m.uz, n, oms, P, shift);
+    auto full = [&](float p) {  // P_i from P_i - shift
+        if constexpr (C::kShiftPoly)
+            return p + shift;
+        else
+            return p;
+    };
     typename C::Elem *const wrow = codec.wr + row + x;
     if (Iind <= 1e-4f) {  // bulk (lbm.cuh:216-247)
         codec.store_bulk(wrow, aR, aB, P);
@@ -574,13 +588,13 @@ __device__ __forceinline__ void collide_node(const Geometry &g, const Physics &p
     t.Ah_absF = ph.Ah * t.absF;
     t.coeff_rho = ph.beta * ((rr * rb) / (rT * rT)) * rT;
     {
-        const float g0 = Dir<0>::w * P[0] + omega2<0>(t);
+        const float g0 = Dir<0>::w * full(P[0]) + omega2<0>(t);
         codec.template store_row<0>(wrow, aR * g0, aB * g0);
     }
     static_for<(kQ - 1) / 2>([&](auto Q) {
         constexpr int i = 2 * decltype(Q)::value + 1;
         const float o2 = omega2<i>(t);  // even: the same for i and its opposite
-        const float gi = Dir<i>::w * P[i] + o2, go = Dir<i + 1>::w * P[i + 1] + o2;
+        const float gi = Dir<i>::w * full(P[i]) + o2, go = Dir<i + 1>::w * full(P[i + 1]) + o2;
         const float d = recolour<i>(t);  // odd: -d for the opposite
         codec.template store_row<i>(wrow, aR * gi + d, aB * gi - d);
         codec.template store_row<i + 1>(wrow, aR * go - d, aB * go + d);

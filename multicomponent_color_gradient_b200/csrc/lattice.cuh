@@ -213,14 +213,15 @@ __device__ __forceinline__ void fneq_pair(const NeqTerms &n, float &fi, float &f
 // <= 2.  D3Q27 is the tensor product of three D1Q3 stencils, so the 27 values
 // follow from the coefficients by three passes of 1-D evaluation at
 // c = -1, 0, 1 (sum factorisation): about 70 adds instead of a Hermite
-// evaluation per direction.
+// evaluation per direction.  `shift` is taken off the constant coefficient,
+// so P[i] comes out as P_i - shift (the float16 store keeps P_i - rho0).
 __device__ __forceinline__ void collision_poly(float rho, float ux, float uy, float uz, const NeqTerms &n, float oms,
-                                               float (&P)[kQ]) {
+                                               float (&P)[kQ], float shift = 0.0f) {
     const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
     const float usq = ux2 + uy2 + uz2;
     const float lin = kInvCs2 - kInv2Cs4 * usq;
     // coefficients of 1, c_a, c_a^2, c_a c_b, c_a^2 c_b, c_x c_y c_z
-    const float a0 = rho - kInv2Cs2 * (rho * usq + oms * (n.pxx + n.pyy + n.pzz));
+    const float a0 = (rho - shift) - kInv2Cs2 * (rho * usq + oms * (n.pxx + n.pyy + n.pzz));
     const float Ax = rho * ux * (lin + kInv6Cs6 * ux2) - oms * kInv2Cs4 * (n.a3xyy + n.a3xzz);
     const float Ay = rho * uy * (lin + kInv6Cs6 * uy2) - oms * kInv2Cs4 * (n.a3xxy + n.a3yzz);
     const float Az = rho * uz * (lin + kInv6Cs6 * uz2) - oms * kInv2Cs4 * (n.a3xxz + n.a3yyz);
