@@ -6,7 +6,7 @@
   peak within 5 %), and Laplace's law dp * R_eff constant across radii.
 * Float16 storage: the 64x128x64 jet crop (D=8, tau 0.52, sigma 0.005) run in
   float32 and float16 storage against the float64 oracle; the radial mean
-  centre-line velocity and half-width agree within 1 % (the north_star bar).
+  centre-line velocity and half-width agree within 1 % (the bar float16 storage is held to).
 """
 import numpy as np
 import pytest

@@ -5,8 +5,8 @@ tests/golden/make_post_fixture.py on a GPU) read back
 * by the reference's own post/mean_profile_io.py (read_metadata,
   read_radial_moments, require_samples, averaged_radial_fields,
   fit_virtual_origin: post/mean_profile_io.py:61-239), imported from the
-  reference checkout when one is present (MCG_REFERENCE_ROOT, default
-  /root/reference), else skipped;
+  reference checkout that MCG_REFERENCE_ROOT names, when one is present,
+  else skipped;
 * by the package's plain-XML replacement of post/binConversionVti.py, which
   needs no vtk package.
 """
