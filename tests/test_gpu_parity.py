@@ -150,7 +150,7 @@ def test_matches_reference_build_small(name, steps, stats_from):
 
 @pytest.mark.parametrize("name,stats_from", [("bubble_64_ref", 10**9), ("jet_128x256x128", 50)])
 def test_matches_reference_build_full_size(name, stats_from):
-    """BASELINE shapes, 100 steps from each code's own initial condition:
+    """The full-size workloads (bubble 64^3, jet 128x256x128), 100 steps from each code's own initial condition:
     max-abs on populations and on psi (the parity measure of the step)."""
     if ref_binary(name) is None:
         pytest.skip("reference build oracle/_ref/ref_%s not present" % name)
