@@ -5,6 +5,8 @@
 // ./JET_VTK/Re<Re>_We<We>/ (or --out DIR) and prints the same MLUPS and tke
 // lines.  Unlike the reference it does not exit on the first CUDA error
 // without a message: every failure prints mcg_last_error_string().
+// `--async_output 1` writes the output steps through mcg_output_step_async:
+// the same files, written by a worker thread while the steps continue.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -43,10 +45,12 @@ int main(int argc, char **argv) {
     mcg_params p;
     mcg_params_default(&p);
     std::string out = ".";
+    bool async_output = false;
     for (int a = 1; a + 1 < argc; a += 2) {
         const std::string k = argv[a];
         if (k.rfind("--", 0) != 0) { std::fprintf(stderr, "bad argument %s\n", argv[a]); return 2; }
         if (k == "--out") { out = argv[a + 1]; continue; }
+        if (k == "--async_output") { async_output = std::atoi(argv[a + 1]) != 0; continue; }
         if (!set_param(p, k.substr(2), argv[a + 1])) { std::fprintf(stderr, "unknown parameter %s\n", argv[a]); return 2; }
     }
     if (!check(mcg_params_derive(&p), "params")) return 1;
@@ -77,9 +81,12 @@ int main(int argc, char **argv) {
                         window_ms, 100.0 * cells / (window_ms * 1e3), double(step) * cells / (total_ms * 1e3));
             window_ms = 0;
         }
-        if (end % p.NOUTPUT == 0)
-            if (!check(mcg_output_step(h, end), "output")) return 1;
+        if (end % p.NOUTPUT == 0) {
+            const mcg_status s = async_output ? mcg_output_step_async(h, end) : mcg_output_step(h, end);
+            if (!check(s, "output")) return 1;
+        }
     }
+    if (!check(mcg_output_flush(h), "output")) return 1;
     if (!check(mcg_write_radial_outputs(h), "radial output")) return 1;
     mcg_destroy(h);
     return 0;

@@ -115,13 +115,15 @@ def test_output_files_match_reference_layout(tmp_path):
     np.testing.assert_allclose(uy_avg[m.ravel()], F["uy"][m.ravel()], rtol=1e-5, atol=1e-7)
 
 
-def test_cpp_driver_runs_the_main_loop(tmp_path):
+@pytest.mark.parametrize("async_output", ["0", "1"])
+def test_cpp_driver_runs_the_main_loop(tmp_path, async_output):
     exe = os.path.join(ROOT, "multicomponent_color_gradient_b200", "bin", "mcg_jet")
     if not os.path.exists(exe):
         pytest.skip("bin/mcg_jet not built")
     out = subprocess.run([exe, "--NX", "24", "--NY", "40", "--NZ", "24", "--jet_radius", "3", "--Re", "45", "--We",
                           "3", "--NSTEP", "200", "--NOUTPUT", "100", "--NSTATS_START_STEP", "50", "--out",
-                          str(tmp_path)], capture_output=True, text=True, timeout=300)
+                          str(tmp_path), "--async_output", async_output], capture_output=True, text=True,
+                         timeout=300)
     assert out.returncode == 0, out.stderr
     assert "MLUPS" in out.stdout and "tke_avg" in out.stdout
     mean = tmp_path / "JET_VTK" / "Re45_We3" / "mean_profiles"
