@@ -13,6 +13,7 @@
 // slots: a third output step waits for the oldest.
 #include <condition_variable>
 #include <deque>
+#include <exception>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -56,15 +57,19 @@ struct AsyncOutput {
             mcg_status st = MCG_OK;
             const cudaError_t e = cudaEventSynchronize(ready[job.slot]);
             if (e != cudaSuccess) st = cuda_fail(e, "asynchronous output copy");
-            if (st == MCG_OK) {
-                tke_update(h, job.step, *h_tke[job.slot]);
-                st = io_write_tke_sample_snap(h, job.step, job.stats);
-            }
-            if (st == MCG_OK && job.radial) st = io_write_radial_host(h, job.stats, h_radial[job.slot]);
-            if (st == MCG_OK && job.vti) {
-                char name[64];
-                std::snprintf(name, sizeof(name), "/lbm_%08d.vti", int(job.step));
-                st = io_write_vti_text(h, h->vti_dir + name, h_text[job.slot]);
+            try {  // an exception (allocation in a writer) becomes the reported error
+                if (st == MCG_OK) {
+                    tke_update(h, job.step, *h_tke[job.slot]);
+                    st = io_write_tke_sample_snap(h, job.step, job.stats);
+                }
+                if (st == MCG_OK && job.radial) st = io_write_radial_host(h, job.stats, h_radial[job.slot]);
+                if (st == MCG_OK && job.vti) {
+                    char name[64];
+                    std::snprintf(name, sizeof(name), "/lbm_%08d.vti", int(job.step));
+                    st = io_write_vti_text(h, h->vti_dir + name, h_text[job.slot]);
+                }
+            } catch (const std::exception &ex) {
+                st = fail(MCG_ERR_IO, std::string("asynchronous output writer: ") + ex.what());
             }
             std::lock_guard<std::mutex> lk(m);
             if (st != MCG_OK && error == MCG_OK) {
