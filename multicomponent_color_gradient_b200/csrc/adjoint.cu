@@ -217,106 +217,110 @@ struct Run {
 extern "C" {
 
 mcg_status mcg_adjoint_plan(int32_t nsteps, int32_t snapshots, int64_t *forward_steps, int32_t *sweeps) {
-    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
-    if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
-    const int free_slots = std::min<int64_t>(snapshots - 1, nsteps);
-    std::vector<Action> acts;
-    plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
-    if (forward_steps) *forward_steps = forward_steps_of(acts);
-    if (sweeps) *sweeps = least_sweeps(int64_t(nsteps) + 1, free_slots + 1);
-    return MCG_OK;
+    return mcg::guarded([&]() -> mcg_status {
+        if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+        if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
+        const int free_slots = std::min<int64_t>(snapshots - 1, nsteps);
+        std::vector<Action> acts;
+        plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
+        if (forward_steps) *forward_steps = forward_steps_of(acts);
+        if (sweeps) *sweeps = least_sweeps(int64_t(nsteps) + 1, free_slots + 1);
+        return MCG_OK;
+    });
 }
 
 mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nsteps, int32_t snapshots, double *J,
                            double *dJ_dsigma, double *dJ_dtau, float *dJ_du0, int64_t *forward_steps, float *ms) {
-    if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
-    if (!psi_target) return fail(MCG_ERR_INVALID_ARG, "psi_target is null");
-    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
-    if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
-    if (h->p.boundary != MCG_BOUNDARY_PERIODIC || h->p.storage != MCG_STORAGE_F32)
-        return fail(MCG_ERR_UNSUPPORTED, "the adjoint covers the periodic box with float32 storage");
-    if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
-    const mcg::Geometry &g = h->s.g;
-    const size_t N = g.N;
-    const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
-    const size_t record_floats = size_t(mcg::kTapePlanes) * N;
-    const bool tape_mode = snapshots > nsteps;
-    const int free_slots = tape_mode ? 0 : snapshots - 1;
+    return mcg::guarded([&]() -> mcg_status {
+        if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+        if (!psi_target) return fail(MCG_ERR_INVALID_ARG, "psi_target is null");
+        if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+        if (snapshots < 1) return fail(MCG_ERR_INVALID_ARG, "snapshots must be >= 1");
+        if (h->p.boundary != MCG_BOUNDARY_PERIODIC || h->p.storage != MCG_STORAGE_F32)
+            return fail(MCG_ERR_UNSUPPORTED, "the adjoint covers the periodic box with float32 storage");
+        if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
+        const mcg::Geometry &g = h->s.g;
+        const size_t N = g.N;
+        const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
+        const size_t record_floats = size_t(mcg::kTapePlanes) * N;
+        const bool tape_mode = snapshots > nsteps;
+        const int free_slots = tape_mode ? 0 : snapshots - 1;
 
-    std::vector<Action> acts;
-    if (!tape_mode) plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
+        std::vector<Action> acts;
+        if (!tape_mode) plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
 
-    DeviceBuffers buf;
-    Run run;
-    run.h = h;
-    run.base = h->s;
-    run.step0 = h->step;
-    run.T = nsteps;
-    run.slots.assign(size_t(free_slots) + 1, nullptr);
-    run.slots[0] = h->s.pops[h->cur];
-    void *p = nullptr;
-    for (int k = 1; k <= free_slots; ++k) {
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint snapshot slots");
-        run.slots[size_t(k)] = p;
-    }
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint work buffers");
-        run.work[k] = p;
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint lambda buffers");
-        run.lam[k] = static_cast<float *>(p);
-    }
-    float *tape = nullptr;
-    if (tape_mode) {
-        ADJ_CUDA(buf.alloc(&p, (size_t(nsteps) + 1) * record_floats * sizeof(float)), "adjoint moment tape");
-        tape = static_cast<float *>(p);
-    } else {
-        ADJ_CUDA(buf.alloc(&p, record_floats * sizeof(float)), "adjoint moment record");
-        run.rec = static_cast<float *>(p);
-        // the moments kernel writes the record: 11 planes, then psi (ghost mirrors unused)
-        run.base.mom = run.rec;
-        run.base.psi[0] = run.base.psi[1] = run.rec + size_t(mcg::kTapePsi) * N;
-    }
-    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment adjoints");
-    run.lmom = static_cast<float *>(p);
-    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint gradient adjoints");
-    run.lf = static_cast<float *>(p);
-    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint du0");
-    float *du0 = static_cast<float *>(p);
-    ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "adjoint target");
-    run.target = static_cast<const float *>(p);
-    ADJ_CUDA(cudaMemcpyAsync(p, psi_target, N * sizeof(float), cudaMemcpyHostToDevice, h->stream), "upload target");
-    ADJ_CUDA(buf.alloc(&p, 4 * sizeof(double)), "adjoint accumulators");
-    run.acc = static_cast<double *>(p);
+        DeviceBuffers buf;
+        Run run;
+        run.h = h;
+        run.base = h->s;
+        run.step0 = h->step;
+        run.T = nsteps;
+        run.slots.assign(size_t(free_slots) + 1, nullptr);
+        run.slots[0] = h->s.pops[h->cur];
+        void *p = nullptr;
+        for (int k = 1; k <= free_slots; ++k) {
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint snapshot slots");
+            run.slots[size_t(k)] = p;
+        }
+        for (int k = 0; k < 2; ++k) {
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint work buffers");
+            run.work[k] = p;
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "adjoint lambda buffers");
+            run.lam[k] = static_cast<float *>(p);
+        }
+        float *tape = nullptr;
+        if (tape_mode) {
+            ADJ_CUDA(buf.alloc(&p, (size_t(nsteps) + 1) * record_floats * sizeof(float)), "adjoint moment tape");
+            tape = static_cast<float *>(p);
+        } else {
+            ADJ_CUDA(buf.alloc(&p, record_floats * sizeof(float)), "adjoint moment record");
+            run.rec = static_cast<float *>(p);
+            // the moments kernel writes the record: 11 planes, then psi (ghost mirrors unused)
+            run.base.mom = run.rec;
+            run.base.psi[0] = run.base.psi[1] = run.rec + size_t(mcg::kTapePsi) * N;
+        }
+        ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "adjoint moment adjoints");
+        run.lmom = static_cast<float *>(p);
+        ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint gradient adjoints");
+        run.lf = static_cast<float *>(p);
+        ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "adjoint du0");
+        float *du0 = static_cast<float *>(p);
+        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "adjoint target");
+        run.target = static_cast<const float *>(p);
+        ADJ_CUDA(cudaMemcpyAsync(p, psi_target, N * sizeof(float), cudaMemcpyHostToDevice, h->stream), "upload target");
+        ADJ_CUDA(buf.alloc(&p, 4 * sizeof(double)), "adjoint accumulators");
+        run.acc = static_cast<double *>(p);
 
-    ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
-    if (tape_mode) {
-        if (mcg_status s = run.run_tape(tape, record_floats)) return s;
-    } else {
-        if (mcg_status s = run.execute(acts)) return s;
-    }
-    // op 0 was the last: its record is S_0's
-    const float *M0 = tape_mode ? tape : run.rec;
-    ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, M0, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
-    ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
-    double acc[3] = {0, 0, 0};
-    ADJ_CUDA(cudaMemcpyAsync(acc, run.acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream), "download J");
-    if (dJ_du0)
-        ADJ_CUDA(cudaMemcpyAsync(dJ_du0, du0, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
-                 "download dJ/du0");
-    ADJ_CUDA(cudaStreamSynchronize(h->stream), "adjoint run");
-    float t_ms = 0.f;
-    ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
+        ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
+        if (tape_mode) {
+            if (mcg_status s = run.run_tape(tape, record_floats)) return s;
+        } else {
+            if (mcg_status s = run.execute(acts)) return s;
+        }
+        // op 0 was the last: its record is S_0's
+        const float *M0 = tape_mode ? tape : run.rec;
+        ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, M0, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
+        ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
+        double acc[3] = {0, 0, 0};
+        ADJ_CUDA(cudaMemcpyAsync(acc, run.acc, sizeof(acc), cudaMemcpyDeviceToHost, h->stream), "download J");
+        if (dJ_du0)
+            ADJ_CUDA(cudaMemcpyAsync(dJ_du0, du0, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+                     "download dJ/du0");
+        ADJ_CUDA(cudaStreamSynchronize(h->stream), "adjoint run");
+        float t_ms = 0.f;
+        ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
 
-    // omega = 1/(1/2 + nu/cs^2) = 1/tau; A/2 = sigma / (8 cs^4 taub)
-    const double omega = h->s.ph.omega, Ah = h->s.ph.Ah;
-    const double tau = h->p.taub;
-    const double dAh_dsigma = 1.0 / (8.0 * double(mcg::kCs4) * tau);
-    if (J) *J = acc[0];
-    if (dJ_dsigma) *dJ_dsigma = acc[2] * dAh_dsigma;
-    if (dJ_dtau) *dJ_dtau = acc[1] * (-omega * omega) + acc[2] * (-Ah / tau);
-    if (forward_steps) *forward_steps = tape_mode ? int64_t(nsteps) : forward_steps_of(acts);
-    if (ms) *ms = t_ms;
-    return MCG_OK;
+        // omega = 1/(1/2 + nu/cs^2) = 1/tau; A/2 = sigma / (8 cs^4 taub)
+        const double omega = h->s.ph.omega, Ah = h->s.ph.Ah;
+        const double tau = h->p.taub;
+        const double dAh_dsigma = 1.0 / (8.0 * double(mcg::kCs4) * tau);
+        if (J) *J = acc[0];
+        if (dJ_dsigma) *dJ_dsigma = acc[2] * dAh_dsigma;
+        if (dJ_dtau) *dJ_dtau = acc[1] * (-omega * omega) + acc[2] * (-Ah / tau);
+        if (forward_steps) *forward_steps = tape_mode ? int64_t(nsteps) : forward_steps_of(acts);
+        if (ms) *ms = t_ms;
+        return MCG_OK;
+    });
 }
 
 
@@ -345,161 +349,163 @@ std::vector<float> bessel_basis(const mcg_params &p) {
 
 mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
                                int32_t segment, double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
-    if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
-    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
-    if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
-        return fail(MCG_ERR_INVALID_ARG, "need 0 <= t_begin <= t_end < nsteps");
-    if (h->p.boundary != MCG_BOUNDARY_JET || h->p.storage != MCG_STORAGE_F32)
-        return fail(MCG_ERR_UNSUPPORTED, "the jet adjoint covers the jet boundary with float32 storage");
-    if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
-    const mcg::Geometry &g = h->s.g;
-    const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
-    const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
-    const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
-    const int nb = mcg::kInletBesselMax;
+    return mcg::guarded([&]() -> mcg_status {
+        if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+        if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+        if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
+            return fail(MCG_ERR_INVALID_ARG, "need 0 <= t_begin <= t_end < nsteps");
+        if (h->p.boundary != MCG_BOUNDARY_JET || h->p.storage != MCG_STORAGE_F32)
+            return fail(MCG_ERR_UNSUPPORTED, "the jet adjoint covers the jet boundary with float32 storage");
+        if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
+        const mcg::Geometry &g = h->s.g;
+        const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
+        const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
+        const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
+        const int nb = mcg::kInletBesselMax;
 
-    DeviceBuffers buf;
-    void *p = nullptr;
-    mcg::DeviceState run = h->s;
-    void *work[2];
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint work buffers");
-        work[k] = p;
-    }
-    // both buffers: slots no kernel rewrites carry their initial values in both
-    ADJ_CUDA(cudaMemcpyAsync(work[0], h->s.pops[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream), "copy state");
-    ADJ_CUDA(cudaMemcpyAsync(work[1], h->s.pops[h->cur ^ 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-             "copy state");
-    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment planes");
-    run.mom = static_cast<float *>(p);
-    ADJ_CUDA(cudaMemcpyAsync(run.mom, h->s.mom, size_t(mcg::kMomCount) * N * sizeof(float), cudaMemcpyDeviceToDevice,
-                             h->stream),
-             "copy moments");
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "jet adjoint psi planes");
-        run.psi[k] = static_cast<float *>(p);
-        ADJ_CUDA(cudaMemcpyAsync(run.psi[k], h->s.psi[k], N * sizeof(float), cudaMemcpyDeviceToDevice, h->stream),
-                 "copy psi");
-    }
-    ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
-    run.bmom = static_cast<float *>(p);
-    // segments of L steps: a snapshot (populations + outlet state) at the
-    // start of each, and a tape of one segment's records
-    const int64_t L = (segment <= 0 || segment >= nsteps) ? nsteps : segment;
-    const int64_t nseg = (nsteps + L - 1) / L;
-    std::vector<void *> snap(size_t(nseg), nullptr);
-    std::vector<float *> snapB(size_t(nseg), nullptr);
-    for (int64_t j = 0; j < nseg; ++j) {
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint snapshots");
-        snap[size_t(j)] = p;
-        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
-        snapB[size_t(j)] = static_cast<float *>(p);
-    }
-    float *tape = nullptr;
-    ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
-    tape = static_cast<float *>(p);
-    float *lam[2];
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint lambda buffers");
-        lam[k] = static_cast<float *>(p);
-    }
-    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment adjoints");
-    float *lmom = static_cast<float *>(p);
-    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "jet adjoint gradient adjoints");
-    float *lf = static_cast<float *>(p);
-    float *LB[2];
-    for (int k = 0; k < 2; ++k) {
-        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint outlet adjoints");
-        LB[k] = static_cast<float *>(p);
-    }
-    const std::vector<float> basis = bessel_basis(h->p);
-    ADJ_CUDA(buf.alloc(&p, basis.size() * sizeof(float)), "jet adjoint profile basis");
-    float *dbasis = static_cast<float *>(p);
-    ADJ_CUDA(cudaMemcpyAsync(dbasis, basis.data(), basis.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
-             "upload profile basis");
-    ADJ_CUDA(buf.alloc(&p, (2 + size_t(nb)) * sizeof(double)), "jet adjoint accumulators");
-    double *acc = static_cast<double *>(p);  // [0] J, [1] (unused), [2..] dJ/dc_k
-    double *dacc_w = nullptr;
-    ADJ_CUDA(buf.alloc(&p, 2 * sizeof(double)), "jet adjoint parameter partials");
-    dacc_w = static_cast<double *>(p);
+        DeviceBuffers buf;
+        void *p = nullptr;
+        mcg::DeviceState run = h->s;
+        void *work[2];
+        for (int k = 0; k < 2; ++k) {
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint work buffers");
+            work[k] = p;
+        }
+        // both buffers: slots no kernel rewrites carry their initial values in both
+        ADJ_CUDA(cudaMemcpyAsync(work[0], h->s.pops[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream), "copy state");
+        ADJ_CUDA(cudaMemcpyAsync(work[1], h->s.pops[h->cur ^ 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                 "copy state");
+        ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment planes");
+        run.mom = static_cast<float *>(p);
+        ADJ_CUDA(cudaMemcpyAsync(run.mom, h->s.mom, size_t(mcg::kMomCount) * N * sizeof(float), cudaMemcpyDeviceToDevice,
+                                 h->stream),
+                 "copy moments");
+        for (int k = 0; k < 2; ++k) {
+            ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "jet adjoint psi planes");
+            run.psi[k] = static_cast<float *>(p);
+            ADJ_CUDA(cudaMemcpyAsync(run.psi[k], h->s.psi[k], N * sizeof(float), cudaMemcpyDeviceToDevice, h->stream),
+                     "copy psi");
+        }
+        ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
+        run.bmom = static_cast<float *>(p);
+        // segments of L steps: a snapshot (populations + outlet state) at the
+        // start of each, and a tape of one segment's records
+        const int64_t L = (segment <= 0 || segment >= nsteps) ? nsteps : segment;
+        const int64_t nseg = (nsteps + L - 1) / L;
+        std::vector<void *> snap(size_t(nseg), nullptr);
+        std::vector<float *> snapB(size_t(nseg), nullptr);
+        for (int64_t j = 0; j < nseg; ++j) {
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint snapshots");
+            snap[size_t(j)] = p;
+            ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
+            snapB[size_t(j)] = static_cast<float *>(p);
+        }
+        float *tape = nullptr;
+        ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
+        tape = static_cast<float *>(p);
+        float *lam[2];
+        for (int k = 0; k < 2; ++k) {
+            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint lambda buffers");
+            lam[k] = static_cast<float *>(p);
+        }
+        ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment adjoints");
+        float *lmom = static_cast<float *>(p);
+        ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "jet adjoint gradient adjoints");
+        float *lf = static_cast<float *>(p);
+        float *LB[2];
+        for (int k = 0; k < 2; ++k) {
+            ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint outlet adjoints");
+            LB[k] = static_cast<float *>(p);
+        }
+        const std::vector<float> basis = bessel_basis(h->p);
+        ADJ_CUDA(buf.alloc(&p, basis.size() * sizeof(float)), "jet adjoint profile basis");
+        float *dbasis = static_cast<float *>(p);
+        ADJ_CUDA(cudaMemcpyAsync(dbasis, basis.data(), basis.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+                 "upload profile basis");
+        ADJ_CUDA(buf.alloc(&p, (2 + size_t(nb)) * sizeof(double)), "jet adjoint accumulators");
+        double *acc = static_cast<double *>(p);  // [0] J, [1] (unused), [2..] dJ/dc_k
+        double *dacc_w = nullptr;
+        ADJ_CUDA(buf.alloc(&p, 2 * sizeof(double)), "jet adjoint parameter partials");
+        dacc_w = static_cast<double *>(p);
 
-    const int64_t step0 = h->step;
-    ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
-    int64_t fwd = 0;
-    // one forward step t of the run's state (work[t & 1] -> work[(t+1) & 1]),
-    // recording into `rec` when given: its psi with the ghost values it reads,
-    // the outlet state before its boundary, and (k_fused) its moments
-    auto forward = [&](int64_t t, float *rec) -> mcg_status {
-        mcg::DeviceState d = run;
-        d.pops[0] = work[t & 1];
-        d.pops[1] = work[(t + 1) & 1];
-        if (rec) {
-            ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
-                                     cudaMemcpyDeviceToDevice, h->stream),
-                     "record psi");
-            ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
-                       "jet adjoint: record outlet state");
-            d.tape = rec;
+        const int64_t step0 = h->step;
+        ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
+        int64_t fwd = 0;
+        // one forward step t of the run's state (work[t & 1] -> work[(t+1) & 1]),
+        // recording into `rec` when given: its psi with the ghost values it reads,
+        // the outlet state before its boundary, and (k_fused) its moments
+        auto forward = [&](int64_t t, float *rec) -> mcg_status {
+            mcg::DeviceState d = run;
+            d.pops[0] = work[t & 1];
+            d.pops[1] = work[(t + 1) & 1];
+            if (rec) {
+                ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
+                                         cudaMemcpyDeviceToDevice, h->stream),
+                         "record psi");
+                ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
+                           "jet adjoint: record outlet state");
+                d.tape = rec;
+            }
+            ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "jet adjoint: forward step");
+            d.tape = nullptr;
+            ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
+            ++fwd;
+            return MCG_OK;
+        };
+        auto save = [&](int64_t j, int64_t t) -> mcg_status {
+            ADJ_CUDA(cudaMemcpyAsync(snap[size_t(j)], work[t & 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                     "save snapshot");
+            ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(run, snapB[size_t(j)], h->stream), "jet adjoint: save outlet");
+            return MCG_OK;
+        };
+        // ---- pass 1 (several segments only): snapshots at every segment start
+        if (mcg_status st = save(0, 0)) return st;
+        if (nseg > 1)
+            for (int64_t t = 0; t < (nseg - 1) * L; ++t) {
+                if (mcg_status st = forward(t, nullptr)) return st;
+                if ((t + 1) % L == 0)
+                    if (mcg_status st = save((t + 1) / L, t + 1)) return st;
+            }
+        // ---- pass 2: per segment from the last, restore, re-run recording, reverse
+        int lc = 0, lb = 0;
+        for (int64_t j = nseg - 1; j >= 0; --j) {
+            const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
+            ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                     "restore snapshot");
+            ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
+                       "jet adjoint: restore outlet");
+            for (int64_t t = s0; t < s1; ++t)
+                if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats)) return st;
+            for (int64_t t = s1 - 1; t >= s0; --t) {
+                const float *rec = tape + size_t(t - s0) * rec_floats;
+                const bool in_window = t >= t_begin && t <= t_end;
+                const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
+                ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
+                           "jet adjoint: collision");
+                ADJ_LAUNCH(h,
+                           mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
+                                                    lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
+                           "jet adjoint: boundary");
+                ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream),
+                           "jet adjoint: moments");
+                lc ^= 1;
+                lb ^= 1;
+            }
         }
-        ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "jet adjoint: forward step");
-        d.tape = nullptr;
-        ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
-        ++fwd;
+        ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
+        std::vector<double> out(2 + size_t(nb));
+        ADJ_CUDA(cudaMemcpyAsync(out.data(), acc, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                 "download J");
+        ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint run");
+        float t_ms = 0.f;
+        ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
+        if (J) *J = out[0];
+        if (dJ_dc)
+            for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
+        if (forward_steps) *forward_steps = fwd;
+        if (ms) *ms = t_ms;
         return MCG_OK;
-    };
-    auto save = [&](int64_t j, int64_t t) -> mcg_status {
-        ADJ_CUDA(cudaMemcpyAsync(snap[size_t(j)], work[t & 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                 "save snapshot");
-        ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(run, snapB[size_t(j)], h->stream), "jet adjoint: save outlet");
-        return MCG_OK;
-    };
-    // ---- pass 1 (several segments only): snapshots at every segment start
-    if (mcg_status st = save(0, 0)) return st;
-    if (nseg > 1)
-        for (int64_t t = 0; t < (nseg - 1) * L; ++t) {
-            if (mcg_status st = forward(t, nullptr)) return st;
-            if ((t + 1) % L == 0)
-                if (mcg_status st = save((t + 1) / L, t + 1)) return st;
-        }
-    // ---- pass 2: per segment from the last, restore, re-run recording, reverse
-    int lc = 0, lb = 0;
-    for (int64_t j = nseg - 1; j >= 0; --j) {
-        const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
-        ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                 "restore snapshot");
-        ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
-                   "jet adjoint: restore outlet");
-        for (int64_t t = s0; t < s1; ++t)
-            if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats)) return st;
-        for (int64_t t = s1 - 1; t >= s0; --t) {
-            const float *rec = tape + size_t(t - s0) * rec_floats;
-            const bool in_window = t >= t_begin && t <= t_end;
-            const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
-            ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
-                       "jet adjoint: collision");
-            ADJ_LAUNCH(h,
-                       mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
-                                                lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
-                       "jet adjoint: boundary");
-            ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream),
-                       "jet adjoint: moments");
-            lc ^= 1;
-            lb ^= 1;
-        }
-    }
-    ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
-    std::vector<double> out(2 + size_t(nb));
-    ADJ_CUDA(cudaMemcpyAsync(out.data(), acc, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
-             "download J");
-    ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint run");
-    float t_ms = 0.f;
-    ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
-    if (J) *J = out[0];
-    if (dJ_dc)
-        for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
-    if (forward_steps) *forward_steps = fwd;
-    if (ms) *ms = t_ms;
-    return MCG_OK;
+    });
 }
 
 }  // extern "C"

@@ -5,6 +5,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -64,6 +66,22 @@ namespace mcg {
 
 // Records the error text for mcg_last_error_string() and returns s.
 mcg_status fail(mcg_status s, const std::string &msg);
+
+// Entry points run their body through guarded(): an exception thrown inside
+// (a host allocation failing) becomes an error status with its message
+// instead of crossing the C ABI.
+template <class F>
+mcg_status guarded(F &&body) noexcept {
+    try {
+        return body();
+    } catch (const std::bad_alloc &) {
+        return fail(MCG_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(MCG_ERR_STATE, e.what());
+    } catch (...) {
+        return fail(MCG_ERR_STATE, "unexpected exception");
+    }
+}
 mcg_status cuda_fail(cudaError_t e, const char *what);
 
 // Radial count materialisation: samples * ncols[rb] on interior y rows.
