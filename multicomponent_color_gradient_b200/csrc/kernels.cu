@@ -68,13 +68,6 @@ struct CodecF32 {
             wrow[slot_pair(i) * NX] = __fmul2_rn(make_float2(aR * Dir<i>::w, aB * Dir<i>::w), make_float2(P[i], P[i]));
         });
     }
-    // pull: `grow` = offset of the source row's group segment
-    template <int I>
-    __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
-        const float2 v = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
-        r = v.x;
-        b = v.y;
-    }
     // pull in two halves: the raw pair at `p` = the source node's element of
     // direction I, then the pair the colour sums add and the total gi
     using Raw = float2;
@@ -152,25 +145,10 @@ struct CodecF16 {
             wrow[slot_pair(i) * NX] = __floats2half2_rn(Ps[i], q);
         });
     }
-    template <int I>
-    __device__ __forceinline__ void load(size_t grow, int xs, float &r, float &b) const {
-        const __half2 h = __ldg(rd + grow + size_t(dir_cx(I) + 1) * NX + xs);
-        f16_decode(h, Dir<I>::w, rho0, r, b);
-    }
-    // total g = fr + fb and difference d = fr - fb of a word: with q the signed
-    // minority fraction, fr - fb = g (1 - q) when red is the majority and
-    // -g (1 + q) otherwise, i.e. g (sign(q) - q)
-    template <int I>
-    __device__ __forceinline__ void load_sd(size_t grow, int xs, float &gs, float &d) const {
-        load_sd_ptr<I>(rd + grow + size_t(dir_cx(I) + 1) * NX + xs, gs, d);
-    }
-    // the same through `p` = the source node's word of direction I
-    template <int I>
-    __device__ __forceinline__ void load_sd_ptr(const __half2 *p, float &gs, float &d) const {
-        const float2 v = decode<I>(__ldg(p), gs);
-        d = v.y;
-    }
-    // pull in two halves: the raw word, then (sum, difference) and the total gi
+    // pull in two halves: the raw word, then the total g = fr + fb and the
+    // difference d = fr - fb.  With q the signed minority fraction, fr - fb =
+    // g (1 - q) when red is the majority and -g (1 + q) otherwise, i.e.
+    // g (sign(q) - q).
     using Raw = __half2;
     template <int I>
     __device__ __forceinline__ Raw load_raw(const __half2 *p) const {
