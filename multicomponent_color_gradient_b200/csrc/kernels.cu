@@ -1642,6 +1642,70 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_terminal(const DeviceState s,
     if (threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(J, r);
 }
 
+// Exponents (a, b, c) of the 17 monomials cx^a cy^b cz^c of the collision
+// polynomial (collision_poly): per-axis degree <= 2, total degree <= 3.
+__host__ __device__ constexpr int poly_exp(int k, int axis) {
+    constexpr int e[17][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {2, 0, 0}, {0, 2, 0},
+                              {0, 0, 2}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {2, 1, 0}, {2, 0, 1},
+                              {1, 2, 0}, {1, 0, 2}, {0, 2, 1}, {0, 1, 2}, {1, 1, 1}};
+    return e[k][axis];
+}
+__host__ __device__ constexpr int ipow1(int c, int e) { return e == 0 ? 1 : (e == 1 ? c : c * c); }
+enum PolyTerm { kT000, kT100, kT010, kT001, kT200, kT020, kT002, kT110, kT101, kT011,
+                kT210, kT201, kT120, kT102, kT021, kT012, kT111 };
+
+// Adjoint of the bulk value g_i = w_i P(c_i) over the collision polynomial's
+// coefficients, from the moments T_k = sum_i v_i m_k(c_i) of per-direction
+// weights v (v = w lambda_g): Phi = (feq polynomial)/rho dotted with T, its
+// u-gradient, and Psi = (fneq polynomial) dotted with T, with the S2 / S3
+// Hermite sums Psi is made of.
+struct PolyAdjoint {
+    float S2[6], S3[7];
+    float Phi, dPhi[3], Psi;
+};
+__device__ __forceinline__ PolyAdjoint poly_adjoint(const float (&T)[17], float ux, float uy, float uz,
+                                                    const NeqTerms &n) {
+    PolyAdjoint r;
+    r.S2[0] = T[kT200] - kCs2 * T[kT000];
+    r.S2[1] = T[kT110];
+    r.S2[2] = T[kT020] - kCs2 * T[kT000];
+    r.S2[3] = T[kT011];
+    r.S2[4] = T[kT002] - kCs2 * T[kT000];
+    r.S2[5] = T[kT101];
+    r.S3[0] = T[kT210] - kCs2 * T[kT010];
+    r.S3[1] = T[kT201] - kCs2 * T[kT001];
+    r.S3[2] = T[kT120] - kCs2 * T[kT100];
+    r.S3[3] = T[kT102] - kCs2 * T[kT100];
+    r.S3[4] = T[kT021] - kCs2 * T[kT001];
+    r.S3[5] = T[kT012] - kCs2 * T[kT010];
+    r.S3[6] = T[kT111];
+    r.Psi = kInv2Cs4 * (n.pxx * r.S2[0] + 2.0f * n.pxy * r.S2[1] + n.pyy * r.S2[2] + 2.0f * n.pyz * r.S2[3] +
+                        n.pzz * r.S2[4] + 2.0f * n.pxz * r.S2[5]) +
+            kInv2Cs6 * (n.a3xxy * r.S3[0] + n.a3xxz * r.S3[1] + n.a3xyy * r.S3[2] + n.a3xzz * r.S3[3] +
+                        n.a3yyz * r.S3[4] + n.a3yzz * r.S3[5] + 2.0f * n.a3xyz * r.S3[6]);
+    // feq_i / (w_i rho) = 1 + q cu + (q^2/2) cu^2 - (q/2) |u|^2 + (q^3/6) cu^3 - (q^2/2) |u|^2 cu, q = 1/cs^2
+    const float usq = ux * ux + uy * uy + uz * uz;
+    const float uTc = ux * T[kT100] + uy * T[kT010] + uz * T[kT001];
+    const float lin = kInvCs2 - kInv2Cs4 * usq;
+    const float t2x = T[kT200] * ux + T[kT110] * uy + T[kT101] * uz;
+    const float t2y = T[kT110] * ux + T[kT020] * uy + T[kT011] * uz;
+    const float t2z = T[kT101] * ux + T[kT011] * uy + T[kT002] * uz;
+    // (1/3) d(cu^3)/du_a summed against T (c^3 = c on the lattice)
+    const float cx3 = ux * ux * T[kT100] + 2.0f * ux * uy * T[kT210] + 2.0f * ux * uz * T[kT201] + uy * uy * T[kT120] +
+                      uz * uz * T[kT102] + 2.0f * uy * uz * T[kT111];
+    const float cy3 = uy * uy * T[kT010] + 2.0f * uy * ux * T[kT120] + 2.0f * uy * uz * T[kT021] + ux * ux * T[kT210] +
+                      uz * uz * T[kT012] + 2.0f * ux * uz * T[kT111];
+    const float cz3 = uz * uz * T[kT001] + 2.0f * uz * ux * T[kT102] + 2.0f * uz * uy * T[kT012] + ux * ux * T[kT201] +
+                      uy * uy * T[kT021] + 2.0f * ux * uy * T[kT111];
+    r.Phi = T[kT000] * (1.0f - kInv2Cs2 * usq) + lin * uTc + kInv2Cs4 * (ux * t2x + uy * t2y + uz * t2z) +
+            kInv6Cs6 * (ux * cx3 + uy * cy3 + uz * cz3);
+    const float q2 = 2.0f * kInv2Cs4, q3h = 3.0f * kInv6Cs6;
+    r.dPhi[0] = -kInvCs2 * ux * T[kT000] - q2 * ux * uTc + lin * T[kT100] + q2 * t2x + q3h * cx3;
+    r.dPhi[1] = -kInvCs2 * uy * T[kT000] - q2 * uy * uTc + lin * T[kT010] + q2 * t2y + q3h * cy3;
+    r.dPhi[2] = -kInvCs2 * uz * T[kT000] - q2 * uz * uTc + lin * T[kT001] + q2 * t2z + q3h * cz3;
+    return r;
+}
+
 // Per node: lambda_post (54 values at the node) -> adjoints of the node's
 // moments (11, to lmom) and colour gradient (3, to lf); float64 partials of
 // dJ/domega (acc[0]) and dJ/d(A/2) (acc[1]).
@@ -1675,7 +1739,6 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
         const NeqTerms n = make_neq(mom[kMomPXX * N + id], mom[kMomPXY * N + id], mom[kMomPYY * N + id],
                                     mom[kMomPYZ * N + id], mom[kMomPZZ * N + id], mom[kMomPXZ * N + id], ux, uy, uz);
-        const float usq = ux * ux + uy * uy + uz * uz;
         const float rho = rr + rb;
         const float invr = 1.0f / rho;
         const float aR = rr * invr, aB = rb * invr;
@@ -1712,94 +1775,79 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         const float invF = has_dir ? 1.0f / absF : 0.0f;
         const float invF2 = invF * invF;
         const float Ah = ph.Ah;
-        float l_d = 0.f, l_rhoeq = 0.f, l_uPx = 0.f, l_uPy = 0.f, l_uPz = 0.f, l_uQ = 0.f, l_oms = 0.f;
-        float S2[6] = {0, 0, 0, 0, 0, 0}, S3[7] = {0, 0, 0, 0, 0, 0, 0};
-        float sAx = 0.f, sAy = 0.f, sAz = 0.f, sB = 0.f, sDx = 0.f, sDy = 0.f, sDz = 0.f, sE = 0.f, sBB = 0.f,
-              l_Ah = 0.f;
         const size_t row = pop_row(g, y, z);
         // (lambda_r, lambda_b) of a direction: one float2, as the populations
         auto lam_at = [&](int slot) {
             return reinterpret_cast<const float2 *>(lam)[row + size_t(slot) * size_t(g.NX) + size_t(x)];
         };
-        {  // rest direction: even only
-            const float2 l0 = lam_at(slot_pair(0));
-            const float lr = l0.x, lb = l0.y;
-            const float lg = aR * lr + aB * lb, ld = lr - lb;
-            const float w = Dir<0>::w;
-            const float E = 1.0f - usq * kInv2Cs2;
-            const float fe = w * rho * E;
-            const float fn = fneq<0>(n);
-            const float o2A = -absF * Dir<0>::B;  // Omega2 / (A/2)
-            const float ge = fe + oms * fn + (interface ? Ah * o2A : 0.0f);
-            l_d += ld * ge;
-            l_rhoeq += lg * fe;
-            l_uQ += lg * w * rho * kInvCs2;
-            l_oms += lg * fn;
-            const float mu = lg * w;
-            S2[0] += mu * Dir<0>::Hxx;
-            S2[2] += mu * Dir<0>::Hyy;
-            S2[4] += mu * Dir<0>::Hzz;
-            if (interface) {
+        // Bulk part: g_i = w_i P(c_i) with P the collision polynomial, so the
+        // sums over directions are the polynomial's coefficients dotted with
+        // the moments T_k = sum_i w_i lambda_g,i m_k(c_i) (and U_k with
+        // lambda_r - lambda_b for the colour split).  The moments are formed
+        // group by group: per (cy, cz) the three cx values reduce to
+        // (sum, sum cx, sum cx^2), which add into the 17 moments with the
+        // weights cy^b cz^c.
+        float Tm[17], Um[17];
+#pragma unroll
+        for (int k = 0; k < 17; ++k) Tm[k] = Um[k] = 0.f;
+        static_for<9>([&](auto G) {
+            constexpr int cy = decltype(G)::value / 3 - 1, cz = decltype(G)::value % 3 - 1;
+            float mv[3], nv[3];
+            static_for<3>([&](auto X) {
+                constexpr int cx = decltype(X)::value - 1;
+                constexpr int i = dir_of(cx, cy, cz);
+                const float2 l = lam_at(slot_pair(i));
+                mv[cx + 1] = Dir<i>::w * (aR * l.x + aB * l.y);
+                nv[cx + 1] = Dir<i>::w * (l.x - l.y);
+            });
+            const float m2 = mv[2] + mv[0], n2 = nv[2] + nv[0];
+            const float ms[3] = {m2 + mv[1], mv[2] - mv[0], m2};
+            const float ns[3] = {n2 + nv[1], nv[2] - nv[0], n2};
+            static_for<17>([&](auto K) {
+                constexpr int k = decltype(K)::value;
+                constexpr int wgt = ipow1(cy, poly_exp(k, 1)) * ipow1(cz, poly_exp(k, 2));
+                constexpr int a = poly_exp(k, 0);
+                if constexpr (wgt == 1) {
+                    Tm[k] += ms[a];
+                    Um[k] += ns[a];
+                } else if constexpr (wgt == -1) {
+                    Tm[k] -= ms[a];
+                    Um[k] -= ns[a];
+                }
+            });
+        });
+        const PolyAdjoint pT = poly_adjoint(Tm, ux, uy, uz, n);
+        const PolyAdjoint pU = poly_adjoint(Um, ux, uy, uz, n);
+        const float(&S2)[6] = pT.S2;
+        const float(&S3)[7] = pT.S3;
+        const float l_rhoeq = rho * pT.Phi;  // sum lambda_g feq (feq is proportional to rho)
+        const float l_oms = pT.Psi;          // sum lambda_g fneq
+        float l_d = rho * pU.Phi + oms * pU.Psi;  // sum (lambda_r - lambda_b) g
+        // interface nodes: the perturbation and recolouring terms, direction by direction
+        float sAx = 0.f, sAy = 0.f, sAz = 0.f, sB = 0.f, sDx = 0.f, sDy = 0.f, sDz = 0.f, sE = 0.f, sBB = 0.f,
+              l_Ah = 0.f;
+        if (interface) {
+            {  // rest direction: even only
+                const float2 l0 = lam_at(slot_pair(0));
+                const float lg = aR * l0.x + aB * l0.y, ld = l0.x - l0.y;
+                const float o2A = -absF * Dir<0>::B;  // Omega2 / (A/2)
+                l_d += ld * (Ah * o2A);
                 sBB += lg * Dir<0>::B;
                 l_Ah += lg * o2A;
             }
-        }
-        static_for<(kQ - 1) / 2>([&](auto P) {
-            constexpr int i = 2 * decltype(P)::value + 1;
-            using D = Dir<i>;
-            const float2 li = lam_at(slot_pair(i)), lo = lam_at(slot_pair(i + 1));
-            const float lri = li.x, lbi = li.y, lro = lo.x, lbo = lo.y;
-            const float lgi = aR * lri + aB * lbi, lgo = aR * lro + aB * lbo;
-            const float ldi = lri - lbi, ldo = lro - lbo;
-            const float gs = lgi + lgo, gd = lgi - lgo, ds = ldi + ldo, dd = ldi - ldo;
-            float cu = 0.f, fc = 0.f;
-            if constexpr (D::cx != 0) { cu += D::fx * ux; fc += D::fx * Fx; }
-            if constexpr (D::cy != 0) { cu += D::fy * uy; fc += D::fy * Fy; }
-            if constexpr (D::cz != 0) { cu += D::fz * uz; fc += D::fz * Fz; }
-            const float wr = D::w * rho;
-            // feq_i = w rho (E + O), feq_o = w rho (E - O)
-            const float E = 1.0f + ((cu * cu) * kInv2Cs4 - usq * kInv2Cs2);
-            const float O = cu * kInvCs2 + cu * ((cu * cu) * kInv6Cs6 - usq * kInv2Cs4);
-            // fneq_i = w (A2 + A3), fneq_o = w (A2 - A3)
-            const float A2 = (n.pxx * D::Hxx + 2.0f * n.pxy * D::Hxy + n.pyy * D::Hyy + 2.0f * n.pyz * D::Hyz +
-                              n.pzz * D::Hzz + 2.0f * n.pxz * D::Hxz) * kInv2Cs4;
-            float A3 = 0.0f;
-            if constexpr (D::Hxxy != 0.0f) A3 += n.a3xxy * D::Hxxy;
-            if constexpr (D::Hxxz != 0.0f) A3 += n.a3xxz * D::Hxxz;
-            if constexpr (D::Hxyy != 0.0f) A3 += n.a3xyy * D::Hxyy;
-            if constexpr (D::Hxzz != 0.0f) A3 += n.a3xzz * D::Hxzz;
-            if constexpr (D::Hyyz != 0.0f) A3 += n.a3yyz * D::Hyyz;
-            if constexpr (D::Hyzz != 0.0f) A3 += n.a3yzz * D::Hyzz;
-            if constexpr (D::Hxyz != 0.0f) A3 += 2.0f * n.a3xyz * D::Hxyz;
-            A3 *= kInv2Cs6;
-            float o2A = 0.0f;  // Omega2 / (A/2), even
-            if (interface) o2A = absF * (D::w * (fc * fc) * invF2 - D::B);
-            const float Ge = wr * E + oms * D::w * A2 + (interface ? Ah * o2A : 0.0f);
-            const float Go = wr * O + oms * D::w * A3;
-            l_d += ds * Ge + dd * Go;
-            l_rhoeq += wr * (gs * E + gd * O);
-            // dfeq/du = w rho (c P - u Q): P = Pe +- Po, Q = 1/cs2 +- cu/cs4
-            const float Pe = kInvCs2 + (cu * cu) * (3.0f * kInv6Cs6) - usq * kInv2Cs4;
-            const float Po = cu * (2.0f * kInv2Cs4);
-            const float cP = wr * (gd * Pe + gs * Po);
-            if constexpr (D::cx != 0) l_uPx += D::fx * cP;
-            if constexpr (D::cy != 0) l_uPy += D::fy * cP;
-            if constexpr (D::cz != 0) l_uPz += D::fz * cP;
-            l_uQ += wr * (gs * kInvCs2 + gd * Po);
-            l_oms += D::w * (gs * A2 + gd * A3);
-            const float me = gs * D::w, mo = gd * D::w;
-            S2[0] += me * D::Hxx; S2[2] += me * D::Hyy; S2[4] += me * D::Hzz;
-            if constexpr (D::Hxy != 0.0f) S2[1] += me * D::Hxy;
-            if constexpr (D::Hyz != 0.0f) S2[3] += me * D::Hyz;
-            if constexpr (D::Hxz != 0.0f) S2[5] += me * D::Hxz;
-            if constexpr (D::Hxxy != 0.0f) S3[0] += mo * D::Hxxy;
-            if constexpr (D::Hxxz != 0.0f) S3[1] += mo * D::Hxxz;
-            if constexpr (D::Hxyy != 0.0f) S3[2] += mo * D::Hxyy;
-            if constexpr (D::Hxzz != 0.0f) S3[3] += mo * D::Hxzz;
-            if constexpr (D::Hyyz != 0.0f) S3[4] += mo * D::Hyyz;
-            if constexpr (D::Hyzz != 0.0f) S3[5] += mo * D::Hyzz;
-            if constexpr (D::Hxyz != 0.0f) S3[6] += mo * D::Hxyz;
-            if (interface) {
+            static_for<(kQ - 1) / 2>([&](auto P) {
+                constexpr int i = 2 * decltype(P)::value + 1;
+                using D = Dir<i>;
+                const float2 li = lam_at(slot_pair(i)), lo = lam_at(slot_pair(i + 1));
+                const float lgi = aR * li.x + aB * li.y, lgo = aR * lo.x + aB * lo.y;
+                const float ldi = li.x - li.y, ldo = lo.x - lo.y;
+                const float gs = lgi + lgo, ds = ldi + ldo, dd = ldi - ldo;
+                float fc = 0.f;
+                if constexpr (D::cx != 0) fc += D::fx * Fx;
+                if constexpr (D::cy != 0) fc += D::fy * Fy;
+                if constexpr (D::cz != 0) fc += D::fz * Fz;
+                const float o2A = absF * (D::w * (fc * fc) * invF2 - D::B);  // Omega2 / (A/2), even
+                l_d += ds * (Ah * o2A);
                 sBB += gs * D::B;
                 l_Ah += gs * o2A;
                 const float a = gs * D::w * fc, d = dd * D::w * D::invc;
@@ -1808,8 +1856,8 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
                 if constexpr (D::cz != 0) { sAz += D::fz * a; sDz += D::fz * d; }
                 sB += a * fc;
                 sE += d * fc;
-            }
-        });
+            });
+        }
         // fneq: Pi enters directly (H2) and through the third-order terms a3
         const float c2 = oms * kInv2Cs4, c3 = oms * kInv2Cs6;
         float lPxx = S2[0] * c2, lPxy = 2.0f * S2[1] * c2, lPyy = S2[2] * c2;
@@ -1825,10 +1873,10 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
         float lux = 2.0f * la_xxy * n.pxy + 2.0f * la_xxz * n.pxz + la_xyy * n.pyy + la_xzz * n.pzz + la_xyz * n.pyz;
         float luy = la_xxy * n.pxx + 2.0f * la_xyy * n.pxy + 2.0f * la_yyz * n.pyz + la_yzz * n.pzz + la_xyz * n.pxz;
         float luz = la_xxz * n.pxx + 2.0f * la_xzz * n.pxz + la_yyz * n.pyy + 2.0f * la_yzz * n.pyz + la_xyz * n.pxy;
-        // feq
-        lux += l_uPx - ux * l_uQ;
-        luy += l_uPy - uy * l_uQ;
-        luz += l_uPz - uz * l_uQ;
+        // feq: rho times the u-gradient of the feq polynomial against T
+        lux += rho * pT.dPhi[0];
+        luy += rho * pT.dPhi[1];
+        luz += rho * pT.dPhi[2];
         // colour gradient: perturbation and recolouring
         float lFx = 0.f, lFy = 0.f, lFz = 0.f, lK = 0.f;
         if (interface) {
