@@ -1980,22 +1980,32 @@ __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, 
     const float invr = 1.0f / rho;
     const float ljx = lux * invr, ljy = luy * invr, ljz = luz * invr;
     lrho -= (lux * ux + luy * uy + luz * uz) * invr;
+    // lambda_g,i = lrho + lj.c_i + lP:H2(c_i) is a quadratic polynomial in c_i:
+    // evaluated at the 27 directions by sum factorisation (per cz, then cy,
+    // then cx) instead of a Hermite sum per direction
+    const float k0 = lrho - kCs2 * (lPxx + lPyy + lPzz);
     const PullMap<CodecF32> pm(g, x, y, z, kPeriodic);
-    static_for<kQ>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        using D = Dir<i>;
-        float lgi = lPxx * D::Hxx + lPyy * D::Hyy + lPzz * D::Hzz;
-        if constexpr (D::Hxy != 0.0f) lgi += lPxy * D::Hxy;
-        if constexpr (D::Hyz != 0.0f) lgi += lPyz * D::Hyz;
-        if constexpr (D::Hxz != 0.0f) lgi += lPxz * D::Hxz;
-        if constexpr (D::cx != 0) lgi += D::fx * ljx;
-        if constexpr (D::cy != 0) lgi += D::fy * ljy;
-        if constexpr (D::cz != 0) lgi += D::fz * ljz;
-        lgi += lrho;
-        size_t grow;
-        int xs;
-        pm.template src<i>(x, grow, xs);
-        reinterpret_cast<float2 *>(lam_out)[grow + size_t(dir_cx(i) + 1) * g.NX + xs] = make_float2(lrr + lgi, lrb + lgi);
+    static_for<3>([&](auto CZ) {
+        constexpr int cz = decltype(CZ)::value - 1;
+        const float az = cz == 0 ? k0 : (cz > 0 ? k0 + ljz + lPzz : k0 - ljz + lPzz);
+        const float bxz = cz == 0 ? ljx : (cz > 0 ? ljx + lPxz : ljx - lPxz);  // coefficient of cx
+        const float byz = cz == 0 ? ljy : (cz > 0 ? ljy + lPyz : ljy - lPyz);  // coefficient of cy
+        static_for<3>([&](auto CY) {
+            constexpr int cy = decltype(CY)::value - 1;
+            const float c0 = cy == 0 ? az : (cy > 0 ? az + byz + lPyy : az - byz + lPyy);
+            const float c1 = cy == 0 ? bxz : (cy > 0 ? bxz + lPxy : bxz - lPxy);
+            const float c2 = c0 + lPxx;
+            static_for<3>([&](auto CX) {
+                constexpr int cx = decltype(CX)::value - 1;
+                constexpr int i = dir_of(cx, cy, cz);
+                const float lgi = cx == 0 ? c0 : (cx > 0 ? c2 + c1 : c2 - c1);
+                size_t grow;
+                int xs;
+                pm.template src<i>(x, grow, xs);
+                reinterpret_cast<float2 *>(lam_out)[grow + size_t(dir_cx(i) + 1) * g.NX + xs] =
+                    make_float2(lrr + lgi, lrb + lgi);
+            });
+        });
     });
 }
 
