@@ -105,3 +105,25 @@ def test_uy_avg_vti_rejects_a_short_file(tmp_path):
         fh.truncate(100)
     with pytest.raises(ValueError, match="expected"):
         write_uy_avg_vti(case)
+
+
+def test_vti_text_several_arrays():
+    """vti_text writes the VTI layout the solver's lbm_*.vti files have: one
+    Float32 point array per name, each base64 of [UInt64 byte count][payload],
+    the first array named as the Scalars attribute."""
+    from multicomponent_color_gradient_b200.post import vti_text
+
+    nx, ny, nz = 3, 4, 2
+    rng = np.random.default_rng(5)
+    arrays = {"rhor": rng.random(nx * ny * nz, dtype=np.float32),
+              "rhob": rng.random(nx * ny * nz, dtype=np.float32)}
+    text = vti_text(nx, ny, nz, arrays)
+    assert text.startswith('<?xml version="1.0"?>\n<VTKFile type="ImageData" version="1.0" '
+                           'byte_order="LittleEndian" header_type="UInt64">\n')
+    assert 'WholeExtent="0 2 0 3 0 1"' in text and '<PointData Scalars="rhor">' in text
+    found = re.findall(r'<DataArray type="Float32" Name="(\w+)" format="binary">\n([A-Za-z0-9+/=]+)\n', text)
+    assert [n for n, _ in found] == ["rhor", "rhob"]
+    for name, b64 in found:
+        raw = base64.b64decode(b64, validate=True)
+        assert struct.unpack("<Q", raw[:8])[0] == len(raw) - 8
+        np.testing.assert_array_equal(np.frombuffer(raw[8:], "<f4"), arrays[name])
