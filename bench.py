@@ -52,17 +52,16 @@ def load_peaks():
 
 
 def traffic_per_launch(cells: int, kernel: str):
-    """DRAM bytes (read + write) of one launch of `kernel` scaled from its
-    committed ncu summary (profiles/<kernel>_jet_*.md, line
-    `dram_bytes_per_node: <value>`), or None."""
-    import glob
-    import re
-
-    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", f"{kernel}_jet_*.md"))):
-        m = re.search(r"dram_bytes_per_node:\s*([0-9.]+)", open(path).read())
-        if m:
-            return int(float(m.group(1)) * cells)
-    return None
+    """DRAM bytes (read + write) of one launch of `kernel` (e.g.
+    "k_fused_pipe<CodecF32>"): the per-node figure of its ncu capture in
+    profiles/traffic.json scaled to `cells` nodes, with the capture it came
+    from; (None, None) when the kernel has no capture there."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            rec = json.load(fh)["kernels"][kernel]
+        return int(float(rec["dram_bytes_per_node"]) * cells), rec.get("workload")
+    except (OSError, KeyError, ValueError):
+        return None, None
 
 
 class ClockSampler:
@@ -267,12 +266,15 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default=DEFAULT_CASE)
     ap.add_argument("--storage", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--repeats", type=int, default=5, help="least number of timed regions of `steps` steps")
+    ap.add_argument("--seconds", type=float, default=1.0, help="least device time over all timed regions")
     ap.add_argument("--no-f16", action="store_true", help="skip the float16-storage companion measurement")
+    ap.add_argument("--s3", type=int, default=1, help="also measure the 256x512x256 jet (float32 and float16)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="host time of the cpu_baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
@@ -298,86 +300,144 @@ def main():
     torch.cuda.set_device(local)
     hbm_peak, peak_kind = load_peaks()
 
-    def measure(storage: str):
+    def measure(storage: str, case_name: str, repeats_min: int, seconds_min: float):
+        """Device time of exactly `args.steps` steps (CUDA events on the solver
+        stream), in several timed regions: at least `repeats_min`, and about
+        `seconds_min` seconds in all so that the clock sampler sees the run.
+        Every rank runs the same number of regions (set from the max over
+        ranks of the first region)."""
         over = {}
         if args.shape:
             over = dict(zip(("NX", "NY", "NZ"), (int(v) for v in args.shape.lower().split("x"))))
-        case = get_case(args.case, storage=storage, NSTATS_START_STEP=0, seed=20260101 + rank, inlet_noise=0.01,
+        case = get_case(case_name, storage=storage, NSTATS_START_STEP=0, seed=20260101 + rank, inlet_noise=0.01,
                         **over)
         S = Solver(case)
         S.init_jet() if case["boundary"] == "jet" else S.init_bubble()
         S.step(args.warmup)
         S.synchronize()
         barrier(world)
-        l0 = S.launches
         sampler = ClockSampler(local)
         sampler.start()
-        ms, per_kernel = S.step_profiled(args.steps)
+        regions, kernel_ms = [], {"fused": 0.0, "boundary": 0.0}
+        launches = n_regions = None
+        while n_regions is None or len(regions) < n_regions:
+            barrier(world)
+            S.synchronize()
+            l0 = S.launches
+            ms, per_kernel = S.step_profiled(args.steps)
+            if launches is None:
+                launches = S.launches - l0
+            for k in kernel_ms:
+                kernel_ms[k] += per_kernel[k]
+            regions.append(max_over_ranks(world, ms))
+            if n_regions is None:
+                n_regions = max(repeats_min, min(200, int(seconds_min * 1e3 / max(regions[0], 1e-3)) + 1))
         clocks = sampler.stop()
-        launches = S.launches - l0
-        ms = max_over_ranks(world, ms)
-        return case, S, ms, per_kernel, launches, clocks
+        cells = case["NX"] * case["NY"] * case["NZ"]
+        ms = float(np.median(regions))
+        step_bytes = 432 if storage == "f32" else 216  # algorithmic bytes per lattice update
+        n_launch = args.steps * len(regions)
+        r = {"case": case, "cells": cells, "ms": ms, "mlups": world * cells * args.steps / (ms * 1e3),
+             "step_bytes": step_bytes, "t_fused": kernel_ms["fused"] / n_launch,
+             "t_bc": kernel_ms["boundary"] / n_launch, "launches": launches, "clocks": clocks,
+             "tiling": S.tiling(),
+             "spread": {"regions": len(regions), "min_ms_per_step": round(min(regions) / args.steps, 6),
+                        "max_ms_per_step": round(max(regions) / args.steps, 6)}}
+        r["achieved"] = step_bytes * cells / (r["t_fused"] * 1e-3) / 1e9  # GB/s of the fused kernel
+        r["step_gbs"] = step_bytes * cells / (ms / args.steps * 1e-3) / 1e9
+        return S, r
 
-    case, S, ms, per_kernel, launches, clocks = measure(args.storage)
-    cells = case["NX"] * case["NY"] * case["NZ"]
-    mlups = world * cells * args.steps / (ms * 1e3)
-    step_bytes = 432 if args.storage == "f32" else 216  # algorithmic bytes per lattice update
-    t_fused = per_kernel["fused"] / args.steps  # ms per launch
-    t_bc = per_kernel["boundary"] / args.steps
-    ach = step_bytes * cells / (t_fused * 1e-3) / 1e9
-    step_gbps = step_bytes * cells / (ms / args.steps * 1e-3) / 1e9
-    tiling = S.tiling()
+    S, m = measure(args.storage, args.case, args.repeats, args.seconds)
+    case, cells, ms, mlups = m["case"], m["cells"], m["ms"], m["mlups"]
+    tiling = m["tiling"]
     kname = "k_fused_pipe" if tiling["pipelined"] else "k_fused"  # the fused-step kernel that ran
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(ach, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(ach / hbm_peak, 4), "peak_kind": peak_kind, "traffic": traffic_per_launch(cells, kname),
-                "algorithmic_bytes_per_node": step_bytes,
-                "step_achieved": round(step_gbps, 1), "step_frac": round(step_gbps / hbm_peak, 4),
+    codec = "CodecF32" if args.storage == "f32" else "CodecF16"
+    traffic, traffic_src = traffic_per_launch(cells, f"{kname}<{codec}>")
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(m["achieved"], 1), "peak": hbm_peak,
+                "unit": "GB/s", "frac": round(m["achieved"] / hbm_peak, 4), "peak_kind": peak_kind,
+                "traffic": traffic, "traffic_capture": traffic_src, "algorithmic_bytes_per_node": m["step_bytes"],
+                "step_achieved": round(m["step_gbs"], 1), "step_frac": round(m["step_gbs"] / hbm_peak, 4),
                 "tiling": tiling,
-                "kernels": {kname: {"ms_per_launch": round(t_fused, 6)},
-                            "k_boundary": {"ms_per_launch": round(t_bc, 6)}}}
+                "kernels": {kname: {"ms_per_launch": round(m["t_fused"], 6)},
+                            "k_boundary": {"ms_per_launch": round(m["t_bc"], 6)}}}
 
-    # end to end through the public API: host state in, K steps, fields out
+    # end to end through the public API: host state in, K steps, fields out,
+    # pinned host buffers on both sides; the job runs three times and the
+    # median is kept
     e2e = None
     try:
         if args.no_e2e:
             raise RuntimeError("skipped (--no-e2e)")
+        keys = ("rhor", "rhob", "ux", "uy", "uz")
         fr_h = torch.empty(27 * cells, dtype=torch.float32, pin_memory=True)
         fb_h = torch.empty(27 * cells, dtype=torch.float32, pin_memory=True)
-        fl_h = {k: torch.empty(cells, dtype=torch.float32, pin_memory=True) for k in ("rhor", "rhob", "ux", "uy", "uz")}
+        fl_h = {k: torch.empty(cells, dtype=torch.float32, pin_memory=True) for k in keys}
+        out_h = {k: torch.empty(cells, dtype=torch.float32, pin_memory=True) for k in keys}
         fr_np, fb_np = S.get_populations()
         fr_h.numpy()[:] = fr_np
         fb_h.numpy()[:] = fb_np
         F = S.get_fields()
-        for k in fl_h:
+        for k in keys:
             fl_h[k].numpy()[:] = F[k]
         del fr_np, fb_np
-        barrier(world)
-        S.synchronize()
-        t0 = time.perf_counter()  # every API call below that returns host data synchronises its stream
-        S.set_fields(**{k: fl_h[k].numpy() for k in fl_h})
-        S.set_populations(fr_h.numpy(), fb_h.numpy())
-        S.step(args.steps)
-        out = S.get_fields()
-        wall = time.perf_counter() - t0
-        e2e_s = max_over_ranks(world, wall)
+        outs = {k: out_h[k].numpy() for k in keys}
+        jobs = []
+        for _ in range(3):
+            barrier(world)
+            S.synchronize()
+            t0 = time.perf_counter()  # every API call below that returns host data synchronises its stream
+            S.set_fields(**{k: fl_h[k].numpy() for k in keys})
+            t1 = time.perf_counter()
+            S.set_populations(fr_h.numpy(), fb_h.numpy())
+            t2 = time.perf_counter()
+            S.step(args.steps)
+            S.synchronize()
+            t3 = time.perf_counter()
+            S.get_fields(out=outs)
+            t4 = time.perf_counter()
+            jobs.append((max_over_ranks(world, t4 - t0), t1 - t0, t2 - t1, t3 - t2, t4 - t3))
+        assert np.isfinite(outs["uy"]).all()
+        jobs.sort()
+        wall, t_fields, t_pops, t_steps, t_out = jobs[len(jobs) // 2]
         h2d = (2 * 27 * cells + 5 * cells) * 4
         d2h = 5 * cells * 4
-        e2e = {"value": round(world * cells * args.steps / (e2e_s * 1e6), 3), "unit": "MLUPS",
+        e2e = {"value": round(world * cells * args.steps / (wall * 1e6), 3), "unit": "MLUPS",
                "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
-               "job": f"upload state ({h2d / 1e6:.0f} MB) + {args.steps} steps + download fields ({d2h / 1e6:.0f} MB)",
-               "seconds": round(e2e_s, 4)}
-        assert np.isfinite(out["uy"]).all()
+               "job": f"upload state ({h2d / 1e6:.0f} MB: 5 fields + 54 populations per node) + {args.steps} steps + "
+                      f"download fields ({d2h / 1e6:.0f} MB), pinned host buffers; median of {len(jobs)} jobs",
+               "seconds": round(wall, 5),
+               "split_ms": {"set_fields": round(t_fields * 1e3, 3), "set_populations": round(t_pops * 1e3, 3),
+                            "steps": round(t_steps * 1e3, 3), "get_fields": round(t_out * 1e3, 3)},
+               "h2d_gbs": round(h2d / (t_fields + t_pops) / 1e9, 2), "d2h_gbs": round(d2h / t_out / 1e9, 2)}
     except Exception as exc:  # keep the device-timed number; report why e2e is missing
         e2e = {"value": None, "unit": "MLUPS", "error": str(exc)[:200]}
     S.close()
 
     f16 = None
     if not args.no_f16 and args.storage == "f32":
-        c16, S16, ms16, pk16, _, _ = measure("f16")
-        m16 = world * cells * args.steps / (ms16 * 1e3)
-        f16 = {"value": round(m16, 3), "unit": "MLUPS", "ratio_vs_f32": round(m16 / mlups, 3),
-               "step_frac_216B": round(216 * cells / (ms16 / args.steps * 1e-3) / 1e9 / hbm_peak, 4)}
+        S16, m16 = measure("f16", args.case, 3, 0.3)
+        f16 = {"value": round(m16["mlups"], 3), "unit": "MLUPS", "ratio_vs_f32": round(m16["mlups"] / mlups, 3),
+               "kernel_frac_216B": round(m16["achieved"] / hbm_peak, 4),
+               "step_frac_216B": round(m16["step_gbs"] / hbm_peak, 4),
+               "kernel_ms_per_launch": round(m16["t_fused"], 6), "tiling": m16["tiling"], "spread": m16["spread"]}
         S16.close()
+
+    s3 = None
+    if args.s3 and not args.shape and args.case == DEFAULT_CASE:
+        s3 = {"workload": "jet_256x512x256", "steps": args.steps}
+        try:
+            for st in ("f32", "f16"):
+                S3, m3 = measure(st, "jet_256x512x256", 3, 0.3)
+                S3.close()
+                s3[st] = {"value": round(m3["mlups"], 3), "unit": "MLUPS",
+                          "kernel_ms_per_launch": round(m3["t_fused"], 6),
+                          "kernel_frac": round(m3["achieved"] / hbm_peak, 4),
+                          "step_frac": round(m3["step_gbs"] / hbm_peak, 4),
+                          "algorithmic_bytes_per_node": m3["step_bytes"], "tiling": m3["tiling"],
+                          "spread": m3["spread"]}
+            s3["f16_ratio_vs_f32"] = round(s3["f16"]["value"] / s3["f32"]["value"], 3)
+        except Exception as exc:
+            s3["error"] = str(exc)[:200]
 
     adjoint = jet_adjoint = None
     if not args.no_adjoint:
@@ -406,9 +466,11 @@ def main():
                    "tau": round(case["taub"], 6), "sigma": round(case["sigma"], 6), "beta": case["beta_recolor"],
                    "radial_statistics": "on", "inlet_noise": 0.01,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (step_bytes / 2 * cells / 1e6)},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-        "f16_store": f16, "adjoint": adjoint, "jet_adjoint": jet_adjoint,
+                   "l2": "inputs larger than L2 (%.0f MB of populations per buffer)" % (m["step_bytes"] / 2 * cells / 1e6)},
+        "timing": {"statistic": "median over timed regions of exactly `steps` steps", **m["spread"]},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m["launches"],
+        "gpu_launches_scope": "per timed region of `steps` steps", "clocks": m["clocks"],
+        "f16_store": f16, "s3": s3, "adjoint": adjoint, "jet_adjoint": jet_adjoint,
     }
     print(json.dumps(line))
 

@@ -232,19 +232,20 @@ mcg_status mcg_check_finite(mcg_handle *h);
 
 /* No counterpart in the reference.  The float64 sums of mcg_conservation_sums
  * for callers that cannot let the library allocate: callers that own all
- * device memory and allow no cudaMalloc/cudaFree inside their time loop (a
- * main.cu-style driver keeping its own LbmDevice buffers with HBM nearly
- * full, where an allocation can fail and a free would synchronise the
- * device).  fr, fb: the caller's device arrays in reference layout
- * f[i*Ncells + id] (Q*Ncells floats each); out5: the caller's device array of
- * 5 doubles (sum fr, sum fb, momentum x,y,z over interior nodes); stream as a
- * cudaStream_t or NULL.  Asynchronous; allocates nothing.  Scratch is one
- * static device array of MCG_STATIC_SCRATCH_PLANES*5 doubles (160 KiB, held by
- * every GPU that loads the library until exit): NZ-2 > MCG_STATIC_SCRATCH_PLANES
- * is rejected with MCG_ERR_INVALID_ARG.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the array:
- * calls whose kernels overlap on the GPU race and must be serialised. */
+ * device memory themselves and allow no cudaMalloc/cudaFree inside their time
+ * loop (HBM nearly full, where an allocation can fail and a free would
+ * synchronise the device).  fr, fb: the caller's device arrays of Q*Ncells
+ * floats each, direction-major, f[i*Ncells + id] with
+ * id = x + NX*(y + NY*z) (ghost shell included); out5: the caller's device
+ * array of 5 doubles (sum fr, sum fb, momentum x,y,z over interior nodes);
+ * stream as a cudaStream_t or NULL.  Asynchronous; allocates nothing.  Scratch
+ * is one static device array of MCG_STATIC_SCRATCH_PLANES*5 doubles (160 KiB,
+ * held by every GPU that loads the library until exit): NZ-2 >
+ * MCG_STATIC_SCRATCH_PLANES is rejected with MCG_ERR_INVALID_ARG.  The first
+ * call on a device (and the first after a device reset) looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * call before any stream capture.  All calls share the array: calls whose
+ * kernels overlap on the GPU race and must be serialised. */
 #define MCG_STATIC_SCRATCH_PLANES 4096
 mcg_status mcg_conservation_sums_static(const float *fr, const float *fb, int32_t NX, int32_t NY, int32_t NZ,
                                         double *out5, void *stream);

@@ -3,6 +3,7 @@
 // Owns device memory behind an opaque handle (the reference's LbmDevice and
 // MeanFieldsDevice, memory.cuh:58-97 and meanF/memoryMeanFields.cuh:57-80),
 // queues work on one stream, returns status codes instead of exiting.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -165,6 +166,12 @@ void release(mcg_handle *h) {
     for (cudaEvent_t e : h->prof_events) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->xfer_start) cudaEventDestroy(h->xfer_start);
+    for (int k = 0; k < 16; ++k) {
+        if (h->xfer_copy[k]) cudaEventDestroy(h->xfer_copy[k]);
+        if (h->xfer_kern[k]) cudaEventDestroy(h->xfer_kern[k]);
+    }
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
 }
 
@@ -355,6 +362,12 @@ mcg_status mcg_create(const mcg_params *p, mcg_handle **out) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreate(&h->ev0);
         if (e == cudaSuccess) e = cudaEventCreate(&h->ev1);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->xfer_start, cudaEventDisableTiming);
+        for (int k = 0; k < 16 && e == cudaSuccess; ++k) {
+            e = cudaEventCreateWithFlags(&h->xfer_copy[k], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->xfer_kern[k], cudaEventDisableTiming);
+        }
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
             const mcg_status s = cuda_fail(e, "mcg_create allocation");
@@ -439,7 +452,7 @@ static mcg_status init_common(mcg_handle *h, int mode) {
                "init fields");
     h->mom_stale = false;
     MCG_LAUNCH(h, mcg::launch_refresh_psi(h->s, h->stream), "init psi");
-    MCG_LAUNCH(h, mcg::launch_init_pops(h->s, mode, nullptr, nullptr, p.init_noise, h->stream), "init populations");
+    MCG_LAUNCH(h, mcg::launch_init_pops(h->s, mode, p.init_noise, h->stream), "init populations");
     return MCG_OK;
 }
 
@@ -464,7 +477,7 @@ mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *r
         MCG_REQUIRE(rhor && rhob && ux && uy && uz, "field pointers must not be null");
         if (mcg_status s = reset_counters(h)) return s;
         if (mcg_status s = mcg_set_fields(h, rhor, rhob, ux, uy, uz)) return s;
-        MCG_LAUNCH(h, mcg::launch_init_pops(h->s, 3, nullptr, nullptr, 0.0f, h->stream), "equilibrium populations");
+        MCG_LAUNCH(h, mcg::launch_init_pops(h->s, 3, 0.0f, h->stream), "equilibrium populations");
         MCG_CUDA(cudaStreamSynchronize(h->stream), "init equilibrium");
         return MCG_OK;
     });
@@ -557,25 +570,61 @@ mcg_status mcg_get_inlet_profile(mcg_handle *h, float *profile) {
 // ---------------------------------------------------------------- state transfer
 
 namespace {
-struct DeviceTemp {
-    void *p = nullptr;
-    ~DeviceTemp() {
-        if (p) cudaFree(p);
-    }
+// Host state transfer in z-chunks of the reference layout, staged in the spare
+// population buffer so that no device memory is allocated: the F32 spare
+// buffer (2*27*N floats) holds every chunk at once, the F16 one (27*N words)
+// half of them, reused in turn.  The host copies of chunk k+1 (copy stream)
+// overlap the scatter or gather kernel of chunk k (solver stream).
+struct XferPlan {
+    int zc = 0, nchunks = 0, slots = 0;
+    size_t pitch = 0;        // elements of one direction row of a chunk
+    size_t slot_floats = 0;  // 2 colours x 27 rows
 };
+
+XferPlan xfer_plan(const mcg_handle *h) {
+    const mcg::Geometry &g = h->s.g;
+    XferPlan x;
+    x.zc = std::max(1, (g.NZ + 7) / 8);
+    x.nchunks = (g.NZ + x.zc - 1) / x.zc;
+    x.pitch = size_t(x.zc) * size_t(g.sz);
+    x.slot_floats = 2 * size_t(mcg::kQ) * x.pitch;
+    const size_t cap = pop_buffer_bytes(h->p) / 4;
+    x.slots = int(std::min<size_t>(size_t(x.nchunks), cap / x.slot_floats));
+    return x;
+}
 }  // namespace
 
 mcg_status mcg_set_populations(mcg_handle *h, const float *fr, const float *fb) {
     return mcg::guarded([&]() -> mcg_status {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(fr && fb, "population pointers must not be null");
-        const size_t n = size_t(mcg::kQ) * h->s.g.N;
-        DeviceTemp t;
-        MCG_CUDA(cudaMalloc(&t.p, 2 * n * 4), "temporary population buffer");
-        float *dfr = static_cast<float *>(t.p), *dfb = dfr + n;
-        MCG_CUDA(cudaMemcpyAsync(dfr, fr, n * 4, cudaMemcpyHostToDevice, h->stream), "upload fr");
-        MCG_CUDA(cudaMemcpyAsync(dfb, fb, n * 4, cudaMemcpyHostToDevice, h->stream), "upload fb");
-        MCG_LAUNCH(h, mcg::launch_init_pops(h->s, 2, dfr, dfb, 0.f, h->stream), "scatter populations");
+        if (mcg_status s = mcg::async_flush(h)) return s;
+        const mcg::Geometry &g = h->s.g;
+        const XferPlan x = xfer_plan(h);
+        if (x.slots < 1 || x.nchunks > 16) return fail(MCG_ERR_STATE, "transfer plan does not fit the spare buffer");
+        const size_t N = g.N;
+        float *stage0 = static_cast<float *>(h->s.pops[1]);
+        const float *src[2] = {fr, fb};
+        // the spare buffer may still be read by queued work of the solver stream
+        MCG_CUDA(cudaEventRecord(h->xfer_start, h->stream), "event record");
+        MCG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->xfer_start, 0), "stream wait");
+        for (int k = 0; k < x.nchunks; ++k) {
+            const int z0 = k * x.zc, nz = std::min(x.zc, g.NZ - z0);
+            float *stage = stage0 + size_t(k % x.slots) * x.slot_floats;
+            if (k >= x.slots) MCG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->xfer_kern[k - x.slots], 0), "stream wait");
+            for (int c = 0; c < 2; ++c)
+                MCG_CUDA(cudaMemcpy2DAsync(stage + size_t(c) * mcg::kQ * x.pitch, x.pitch * 4, src[c] + size_t(z0) * g.sz,
+                                           N * 4, size_t(nz) * g.sz * 4, mcg::kQ, cudaMemcpyHostToDevice,
+                                           h->copy_stream),
+                         "upload populations");
+            MCG_CUDA(cudaEventRecord(h->xfer_copy[k], h->copy_stream), "event record");
+            MCG_CUDA(cudaStreamWaitEvent(h->stream, h->xfer_copy[k], 0), "stream wait");
+            MCG_LAUNCH(h, mcg::launch_scatter_chunk(h->s, 0, stage, x.pitch, z0, nz, h->stream), "scatter populations");
+            MCG_CUDA(cudaEventRecord(h->xfer_kern[k], h->stream), "event record");
+        }
+        // both buffers carry the same ghost-plane slots (the ones no step rewrites)
+        MCG_CUDA(cudaMemcpyAsync(h->s.pops[1], h->s.pops[0], pop_buffer_bytes(h->p), cudaMemcpyDeviceToDevice, h->stream),
+                 "copy populations");
         h->cur = 0;
         MCG_CUDA(cudaStreamSynchronize(h->stream), "set populations");
         return MCG_OK;
@@ -586,13 +635,33 @@ mcg_status mcg_get_populations(mcg_handle *h, float *fr, float *fb) {
     return mcg::guarded([&]() -> mcg_status {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(fr && fb, "population pointers must not be null");
-        const size_t n = size_t(mcg::kQ) * h->s.g.N;
-        DeviceTemp t;
-        MCG_CUDA(cudaMalloc(&t.p, 2 * n * 4), "temporary population buffer");
-        float *dfr = static_cast<float *>(t.p), *dfb = dfr + n;
-        MCG_LAUNCH(h, mcg::launch_gather_pops(h->s, h->cur, dfr, dfb, h->stream), "gather populations");
-        MCG_CUDA(cudaMemcpyAsync(fr, dfr, n * 4, cudaMemcpyDeviceToHost, h->stream), "download fr");
-        MCG_CUDA(cudaMemcpyAsync(fb, dfb, n * 4, cudaMemcpyDeviceToHost, h->stream), "download fb");
+        if (mcg_status s = mcg::async_flush(h)) return s;
+        const mcg::Geometry &g = h->s.g;
+        const XferPlan x = xfer_plan(h);
+        if (x.slots < 1 || x.nchunks > 16) return fail(MCG_ERR_STATE, "transfer plan does not fit the spare buffer");
+        const size_t N = g.N;
+        const int rd = h->cur;
+        float *stage0 = static_cast<float *>(h->s.pops[rd ^ 1]);
+        float *dst[2] = {fr, fb};
+        for (int k = 0; k < x.nchunks; ++k) {
+            const int z0 = k * x.zc, nz = std::min(x.zc, g.NZ - z0);
+            float *stage = stage0 + size_t(k % x.slots) * x.slot_floats;
+            if (k >= x.slots) MCG_CUDA(cudaStreamWaitEvent(h->stream, h->xfer_copy[k - x.slots], 0), "stream wait");
+            MCG_LAUNCH(h, mcg::launch_gather_chunk(h->s, rd, stage, x.pitch, z0, nz, h->stream), "gather populations");
+            MCG_CUDA(cudaEventRecord(h->xfer_kern[k], h->stream), "event record");
+            MCG_CUDA(cudaStreamWaitEvent(h->copy_stream, h->xfer_kern[k], 0), "stream wait");
+            for (int c = 0; c < 2; ++c)
+                MCG_CUDA(cudaMemcpy2DAsync(dst[c] + size_t(z0) * g.sz, N * 4, stage + size_t(c) * mcg::kQ * x.pitch,
+                                           x.pitch * 4, size_t(nz) * g.sz * 4, mcg::kQ, cudaMemcpyDeviceToHost,
+                                           h->copy_stream),
+                         "download populations");
+            MCG_CUDA(cudaEventRecord(h->xfer_copy[k], h->copy_stream), "event record");
+        }
+        // the spare buffer again holds the ghost-plane slots of the current one
+        MCG_CUDA(cudaStreamWaitEvent(h->stream, h->xfer_copy[x.nchunks - 1], 0), "stream wait");
+        MCG_CUDA(cudaMemcpyAsync(h->s.pops[rd ^ 1], h->s.pops[rd], pop_buffer_bytes(h->p), cudaMemcpyDeviceToDevice,
+                                 h->stream),
+                 "restore spare buffer");
         MCG_CUDA(cudaStreamSynchronize(h->stream), "get populations");
         return MCG_OK;
     });

@@ -52,6 +52,11 @@ struct mcg_handle {
     std::vector<float> inlet_coeffs;    // the Bessel coefficients it was made from
     double *d_scalar = nullptr;  // 8 doubles of device scratch for reductions
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // host state transfer (mcg_set/get_populations): a copy stream beside
+    // `stream`, and per z-chunk events of the copies and of the kernels
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t xfer_start = nullptr;
+    cudaEvent_t xfer_copy[16] = {}, xfer_kern[16] = {};
     std::vector<cudaEvent_t> prof_events;  // mcg_step_profiled
 
     mcg::AsyncOutput *async_out = nullptr;  // mcg_output_step_async pipeline (created on first use)

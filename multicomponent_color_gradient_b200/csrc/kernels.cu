@@ -25,7 +25,6 @@
 // populations a reference step never rewrites (y=1 slots fed by non-jet
 // inlet columns, y=NY-2 slots fed by ghost columns) are ghost-plane values of
 // both buffers that no kernel writes, so results are the same.
-#include <cooperative_groups.h>
 #include <type_traits>
 #include <cuda_fp16.h>
 
@@ -38,7 +37,6 @@
 namespace mcg {
 namespace {
 
-namespace cg = cooperative_groups;
 constexpr unsigned kFull = 0xffffffffu;
 
 // ------------------------------------------------------------------ storage codecs
@@ -640,30 +638,6 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
 
 constexpr int kFusedThreads = 256;
 
-// L2 prefetch of the populations that node row (y, z) pulls: one bulk
-// prefetch (cp.async.bulk.prefetch.L2, no shared memory, no completion to wait
-// for) per (cy, cz) group segment of its nine source rows.  `k` in [0, 9)
-// picks the group.  Rows whose pull does not happen (a y ghost row of the
-// closed or jet box) are skipped; sources follow the same wrap and ghost rules
-// as PullMap, so every address lies inside the buffer.
-template <class C, bool kPeriodic>
-__device__ __forceinline__ void prefetch_pull_group(const Geometry &g, const C &codec, int y, int z, int k) {
-    int yn = y, zn = z;
-    if constexpr (kPeriodic) {
-        yn = wrap_interior(y, g.NY);
-        zn = wrap_interior(z, g.NZ);
-    } else {
-        if (y < 1 || y > g.NY - 2 || z < 1 || z > g.NZ - 2) return;
-    }
-    const int cy = k / 3 - 1, cz = k % 3 - 1;
-    int ys = yn - cy, zs = zn - cz;
-    const bool ghost = !kPeriodic && (ys == 0 || ys == g.NY - 1);
-    if (kPeriodic) ys = wrap_interior(ys, g.NY);
-    if (!ghost) zs = wrap_interior(zs, g.NZ);
-    const typename C::Elem *p = codec.rd + pop_row(g, ys, zs) + size_t(k * C::kGroupSlots) * size_t(g.NX);
-    const uint32_t bytes = uint32_t(C::kGroupSlots * g.NX * sizeof(typename C::Elem));
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 #ifndef MCG_FUSED_MIN_BLOCKS
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
@@ -885,17 +859,6 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     const C codec = fused_codec<C, kNX>(s_arg, cur);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
-    // Cluster of consecutive y-tiles (same z-chunk): a tile takes its halo
-    // rows from its neighbours' shared memory instead of pulling them.  Every
-    // CTA of a cluster runs the same number of planes, so the cluster
-    // barriers below are reached the same number of times by all of them.
-    cg::cluster_group cluster = cg::this_cluster();
-    const int crank = T.cluster > 1 ? int(cluster.block_rank()) : 0;
-    const bool lower_nbr = T.cluster > 1 && crank > 0;
-    const bool upper_nbr = T.cluster > 1 && crank < T.cluster - 1;
-    const float *nbr_lo = lower_nbr ? cluster.map_shared_rank(ring, crank - 1) : nullptr;
-    const float *nbr_hi = upper_nbr ? cluster.map_shared_rank(ring, crank + 1) : nullptr;
-
     // Odd chunks march down: the plane two neighbouring chunks both pull (one
     // as its halo, one as its own) is then pulled by both at the same end of
     // their marches, close in time, and the second pull finds it in L2.
@@ -905,30 +868,10 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         float *ringp = ring + (zp % 3) * pstride;
         float *msmp = msm + (zp & 1) * mplane;
         const bool own_plane = zp >= z0 && zp < z0 + lz;
-        if (T.prefetch > 0) {
-            // the rows of the plane `prefetch` steps ahead that this tile will pull
-            const int zf = down ? zp - T.prefetch : zp + T.prefetch;
-            const int nseg = 9 * (ty + 2);
-            if (zf >= z0 - 1 && zf <= z0 + lz && int(threadIdx.x) < nseg)
-                prefetch_pull_group<C, kPeriodic>(g, codec, y0 - 1 + int(threadIdx.x) / 9, zf, int(threadIdx.x) % 9);
-        }
         // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
         for (int r = lr; r < ty + 2; r += rpt) {
-            if ((r == 0 && lower_nbr) || (r == ty + 1 && upper_nbr)) continue;  // from a neighbour below
             tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
                                             ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
-        }
-        if (T.cluster > 1) {
-            // own rows of plane zp are now visible cluster-wide; copy the
-            // neighbours' edge rows into this tile's halo rows.  A neighbour
-            // rewrites this ring slot only three planes later, after two more
-            // cluster barriers that this CTA has not reached yet.
-            cluster.sync();
-            const int off = (zp % 3) * pstride;
-            for (int i = threadIdx.x; i < g.NX; i += kFusedThreads) {
-                if (lower_nbr) ringp[i] = nbr_lo[off + T.ty * tpr + i];
-                if (upper_nbr) ringp[(ty + 1) * tpr + i] = nbr_hi[off + tpr + i];
-            }
         }
         __syncthreads();
         // ---- relax the plane behind the march front, whose neighbours are all pulled
@@ -945,8 +888,6 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         }
         __syncthreads();
     }
-    // no CTA leaves while a neighbour may still read its shared memory
-    if (T.cluster > 1) cluster.sync();
 }
 
 // ------------------------------------------------------------------ software-pipelined fused step
@@ -1278,7 +1219,7 @@ __global__ void k_init_fields(const DeviceState s, int mode, int red_inside, flo
 // Populations of every interior node, written at their pull sources in both
 // buffers (so slots no kernel rewrites hold the initial value in both).
 template <class C>
-__global__ void k_init_pops(const DeviceState s, int mode, const float *fr_ref, const float *fb_ref, float noise) {
+__global__ void k_init_pops(const DeviceState s, int mode, float noise) {
     const Geometry &g = s.g;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -1291,10 +1232,7 @@ __global__ void k_init_pops(const DeviceState s, int mode, const float *fr_ref, 
     const float usq = ux * ux + uy * uy + uz * uz;
     for (int i = 0; i < kQ; ++i) {
         float fr, fb;
-        if (mode == 2) {
-            fr = fr_ref[size_t(i) * N + id];
-            fb = fb_ref[size_t(i) * N + id];
-        } else if (mode == 3) {
+        if (mode == 3) {
             // per colour, the third-order equilibrium at the node's velocity (lbm.cuh:16-35)
             const float cu = float(dir_cx(i)) * ux + float(dir_cy(i)) * uy + float(dir_cz(i)) * uz;
             const float A2 = (cu * cu) * kInv2Cs4 - usq * kInv2Cs2 + cu * kInvCs2;
@@ -1341,25 +1279,52 @@ __global__ void k_refresh_psi(const DeviceState s) {
     s.psi[1][id] = p;
 }
 
+// Host state transfer in z-chunks of the reference layout f[i*Ncells + id].
+// A chunk holds planes [z0, z0 + nz) of both colours, staged as
+// stage[colour][i][id - z0*NX*NY] with `pitch` elements per direction row, so
+// that the host copy of each colour is one 2-D copy of 27 rows.
+//
+// Scatter: the populations of the chunk's interior nodes go to their pull
+// sources in buffer `wbuf` (the sources of planes z0 and z0+nz-1 lie in the
+// neighbouring chunks' planes; every source is written by exactly one node).
 template <class C>
-__global__ void k_gather_pops(const DeviceState s, int cur, float *fr_ref, float *fb_ref) {
+__global__ void k_scatter_chunk(const DeviceState s, int wbuf, const float *__restrict__ stage, size_t pitch, int z0) {
     const Geometry &g = s.g;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    if (x >= g.NX || y >= g.NY) return;
-    const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
-    const size_t N = g.N;
-    const bool interior = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
+    const int z = z0 + int(blockIdx.z);
+    if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
+    const size_t lid = size_t(x) + size_t(g.sy) * size_t(y) + size_t(g.sz) * size_t(blockIdx.z);
+    const float *fr = stage, *fb = stage + size_t(kQ) * pitch;
     for (int i = 0; i < kQ; ++i) {
-        float fr = 0.0f, fb = 0.0f;
+        int xs, ys, zs;
+        pull_src_rt(g, x, y, z, i, xs, ys, zs);
+        C::store_to(s.pops[wbuf], g, i, xs, ys, zs, fr[size_t(i) * pitch + lid], fb[size_t(i) * pitch + lid],
+                    s.ph.f16_rho0);
+    }
+}
+
+// Gather: f(t) = pops[cur] pulled at the chunk's nodes into the stage; ghost
+// nodes give 0.
+template <class C>
+__global__ void k_gather_chunk(const DeviceState s, int cur, float *__restrict__ stage, size_t pitch, int z0) {
+    const Geometry &g = s.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = z0 + int(blockIdx.z);
+    if (x >= g.NX || y >= g.NY) return;
+    const size_t lid = size_t(x) + size_t(g.sy) * size_t(y) + size_t(g.sz) * size_t(blockIdx.z);
+    const bool interior = x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
+    float *fr = stage, *fb = stage + size_t(kQ) * pitch;
+    for (int i = 0; i < kQ; ++i) {
+        float r = 0.0f, b = 0.0f;
         if (interior) {
             int xs, ys, zs;
             pull_src_rt(g, x, y, z, i, xs, ys, zs);
-            C::load_from(s.pops[cur], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
+            C::load_from(s.pops[cur], g, i, xs, ys, zs, r, b, s.ph.f16_rho0);
         }
-        fr_ref[size_t(i) * N + id] = fr;
-        fb_ref[size_t(i) * N + id] = fb;
+        fr[size_t(i) * pitch + lid] = r;
+        fb[size_t(i) * pitch + lid] = b;
     }
 }
 
@@ -1506,19 +1471,9 @@ cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur,
             <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
         return cudaGetLastError();
     }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(t.ny_tiles, t.nz_chunks);
-    cfg.blockDim = dim3(kFusedThreads);
-    cfg.dynamicSmemBytes = size_t(t.smem_bytes);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = unsigned(t.cluster);
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_fused<C, kStats, kPeriodic, kNX>, s, t, cur, step);
+    k_fused<C, kStats, kPeriodic, kNX>
+        <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
+    return cudaGetLastError();
 }
 
 template <class C, bool kStats, bool kPeriodic>
@@ -2334,15 +2289,6 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     if (ty > rpt) ty -= ty % rpt;  // whole rounds of rows in parallel
     t.ty = ty;
     t.ny_tiles = (g.NY - 2 + ty - 1) / ty;
-    // y-tiles per cluster: 1 by default (measured: sharing halo rows through
-    // distributed shared memory cost more in cluster barriers than it saved in
-    // pulls on 128x256x128); the cluster path stays selectable for tuning
-    t.cluster = 1;
-    if (const char *v = std::getenv("MCG_FUSED_CLUSTER")) {  // tuning sweeps
-        const int c = std::atoi(v);
-        if (c >= 1 && c <= 8 && t.ny_tiles % c == 0) t.cluster = c;
-    }
-
     // z chunks: about seven CTAs per SM over the launch (measured best: 8-plane
     // chunks, 1024 CTAs on 128x256x128)
     const int target = 7 * 148;
@@ -2361,14 +2307,8 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
     t.lz = lz;
     t.nz_chunks = (g.NZ - 2 + lz - 1) / lz;
-    if (t.cluster > 1) t.pipe = 0;
     t.smem_bytes = t.pipe ? (kPipeRing * (ty + 2) + kPipeStage * kMomCount * ty) * per_row
                           : (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
-    // bulk prefetch needs 16-byte aligned segments of a multiple of 16 bytes:
-    // NX even (float32 rows of 6 NX floats) or a multiple of 4 (float16, 3 NX words)
-    t.prefetch = 0;
-    if (const char *v = std::getenv("MCG_FUSED_PREFETCH")) t.prefetch = std::max(0, std::atoi(v));  // tuning sweeps
-    if (g.NX % (g.storage == kStoreF16 ? 4 : 2) != 0) t.prefetch = 0;
     t.alternate = 1;
     if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
     // compile-time row length for rows of exactly kFusedNX columns (measured
@@ -2432,12 +2372,11 @@ cudaError_t launch_init_fields(const DeviceState &s, int mode, int red_inside, f
     return cudaGetLastError();
 }
 
-cudaError_t launch_init_pops(const DeviceState &s, int mode, const float *fr_ref, const float *fb_ref, float noise,
-                             cudaStream_t st) {
+cudaError_t launch_init_pops(const DeviceState &s, int mode, float noise, cudaStream_t st) {
     if (s.g.storage == kStoreF16)
-        k_init_pops<CodecF16><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, mode, fr_ref, fb_ref, noise);
+        k_init_pops<CodecF16><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, mode, noise);
     else
-        k_init_pops<CodecF32><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, mode, fr_ref, fb_ref, noise);
+        k_init_pops<CodecF32><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, mode, noise);
     return cudaGetLastError();
 }
 
@@ -2446,11 +2385,25 @@ cudaError_t launch_refresh_psi(const DeviceState &s, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather_pops(const DeviceState &s, int cur, float *fr_ref, float *fb_ref, cudaStream_t st) {
+cudaError_t launch_scatter_chunk(const DeviceState &s, int wbuf, const float *stage, size_t pitch, int z0, int nz,
+                                 cudaStream_t st) {
+    dim3 grid = grid3(s.g);
+    grid.z = unsigned(nz);
     if (s.g.storage == kStoreF16)
-        k_gather_pops<CodecF16><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, cur, fr_ref, fb_ref);
+        k_scatter_chunk<CodecF16><<<grid, dim3(kBX, kBY), 0, st>>>(s, wbuf, stage, pitch, z0);
     else
-        k_gather_pops<CodecF32><<<grid3(s.g), dim3(kBX, kBY), 0, st>>>(s, cur, fr_ref, fb_ref);
+        k_scatter_chunk<CodecF32><<<grid, dim3(kBX, kBY), 0, st>>>(s, wbuf, stage, pitch, z0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_chunk(const DeviceState &s, int cur, float *stage, size_t pitch, int z0, int nz,
+                                cudaStream_t st) {
+    dim3 grid = grid3(s.g);
+    grid.z = unsigned(nz);
+    if (s.g.storage == kStoreF16)
+        k_gather_chunk<CodecF16><<<grid, dim3(kBX, kBY), 0, st>>>(s, cur, stage, pitch, z0);
+    else
+        k_gather_chunk<CodecF32><<<grid, dim3(kBX, kBY), 0, st>>>(s, cur, stage, pitch, z0);
     return cudaGetLastError();
 }
 

@@ -78,15 +78,11 @@ struct Physics {
 // Tiling of the fused step: a CTA owns rows [y0, y0+ty) of every plane of a
 // z-chunk [z0, z0+lz) and marches z (up, or down for odd chunks when
 // `alternate`); tpr threads per row (a multiple of 32,
-// >= NX), blockDim.x / tpr rows in parallel.  `cluster` consecutive y-tiles
-// form a thread-block cluster that exchanges edge psi rows through
-// distributed shared memory, so only the cluster's outer halo rows are pulled.
+// >= NX), blockDim.x / tpr rows in parallel.
 struct FusedTiling {
     int ty, lz, tpr;
     int ny_tiles, nz_chunks;
-    int cluster;
     int smem_bytes;
-    int prefetch;  // planes ahead whose source rows are prefetched into L2 (0: off)
     int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
     int pipe;      // software-pipelined march (k_fused_pipe): one barrier per plane
     int fixed_nx;  // row length the kernel is compiled for (0: runtime geometry)
@@ -126,16 +122,21 @@ cudaError_t launch_boundary(const DeviceState &s, int wbuf, int64_t step, int wh
 cudaError_t launch_accumulate_radial(const DeviceState &s, cudaStream_t st);
 
 // Initial state.  mode 0: jet (jet/jetIn.cuh), 1: bubble (bubble/bubbleIn.cuh),
-// 2: populations from reference-layout device arrays fr_ref/fb_ref,
 // 3: per-colour equilibrium feq(rho_c, u) of the moment planes rr, rb, u.
 cudaError_t launch_init_fields(const DeviceState &s, int mode, int red_inside, float bubble_r2, float bx, float by,
                                float bz, cudaStream_t st);
-cudaError_t launch_init_pops(const DeviceState &s, int mode, const float *fr_ref, const float *fb_ref, float noise,
-                             cudaStream_t st);
+cudaError_t launch_init_pops(const DeviceState &s, int mode, float noise, cudaStream_t st);
 // psi of both buffers from the density planes, all nodes (periodic: ghosts mirrored).
 cudaError_t launch_refresh_psi(const DeviceState &s, cudaStream_t st);
-// Reference-layout gather of f(t) = pops[cur] pulled, interior nodes; ghosts 0.
-cudaError_t launch_gather_pops(const DeviceState &s, int cur, float *fr_ref, float *fb_ref, cudaStream_t st);
+// Host state transfer by z-chunks of the reference layout f[i*Ncells + id]:
+// `stage` holds planes [z0, z0+nz) of both colours as
+// stage[colour][i][id - z0*NX*NY], `pitch` elements per direction row.
+// Scatter: the chunk's interior populations to their pull sources in
+// pops[wbuf].  Gather: f(t) = pops[cur] pulled at the chunk's nodes (ghosts 0).
+cudaError_t launch_scatter_chunk(const DeviceState &s, int wbuf, const float *stage, size_t pitch, int z0, int nz,
+                                 cudaStream_t st);
+cudaError_t launch_gather_chunk(const DeviceState &s, int cur, float *stage, size_t pitch, int z0, int nz,
+                                cudaStream_t st);
 
 // Diagnostics / mean fields.
 cudaError_t launch_tke(const DeviceState &s, double *out, cudaStream_t st);

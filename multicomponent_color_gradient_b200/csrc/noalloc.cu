@@ -86,48 +86,97 @@ __global__ void __launch_bounds__(kThreads) k_fold_planes(const double *partials
 }
 
 std::mutex g_setup_mutex;
-double *g_partials_addr[kMaxDevices] = {};
+struct ScratchAddr {
+    void *ctx = nullptr;  // the context the address belongs to
+    double *ptr = nullptr;
+};
+ScratchAddr g_partials_addr[kMaxDevices];
+
+// cuCtxGetCurrent through the runtime's driver entry point table (the library
+// does not link libcuda itself, so that it loads on machines without a GPU).
+using CtxGetCurrent = int (*)(void **);
+CtxGetCurrent ctx_get_current() {
+    static CtxGetCurrent fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return CtxGetCurrent(nullptr);
+        }
+        return reinterpret_cast<CtxGetCurrent>(f);
+    }();
+    return fn;
+}
+
+void *current_context() {
+    void *ctx = nullptr;
+    if (CtxGetCurrent f = ctx_get_current()) f(&ctx);
+    return ctx;
+}
 
 // Device address of g_static_partials on the current device.  The host-side
 // name is only a stand-in for the symbol; the address comes from
-// cudaGetSymbolAddress, once per device, with that device current.
+// cudaGetSymbolAddress with that device current, once per device and
+// context: a cudaDeviceReset tears the context and its module down, and the
+// next context may load the array elsewhere, so a change of the current
+// context looks the address up again.
 mcg_status scratch_on_current_device(double **out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return mcg::cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return mcg::fail(MCG_ERR_UNSUPPORTED, "device index beyond 64");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_addr[dev]) {
+    ScratchAddr &a = g_partials_addr[dev];
+    void *ctx = current_context();
+    if (!a.ptr || !ctx || ctx != a.ctx) {
         void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_partials);
-        if (e != cudaSuccess) return mcg::cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
-        g_partials_addr[dev] = static_cast<double *>(p);
+        e = cudaGetSymbolAddress(&p, g_static_partials);  // initialises the context if needed
+        if (e != cudaSuccess) {
+            a = ScratchAddr{};
+            return mcg::cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+        }
+        a.ptr = static_cast<double *>(p);
+        a.ctx = current_context();
     }
-    *out = g_partials_addr[dev];
+    *out = a.ptr;
     return MCG_OK;
+}
+
+void forget_scratch_on_current_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    g_partials_addr[dev] = ScratchAddr{};
 }
 
 }  // namespace
 
 extern "C" mcg_status mcg_conservation_sums_static(const float *fr, const float *fb, int32_t NX, int32_t NY,
                                                    int32_t NZ, double *out5, void *stream) {
-    if (!fr || !fb || !out5) return mcg::fail(MCG_ERR_INVALID_ARG, "fr, fb and out5 must be device pointers");
-    if (NX < 3 || NY < 3 || NZ < 3) return mcg::fail(MCG_ERR_INVALID_ARG, "NX, NY, NZ must be >= 3");
-    const int planes = NZ - 2;
-    if (planes > MCG_STATIC_SCRATCH_PLANES)
-        return mcg::fail(MCG_ERR_INVALID_ARG, "NZ - 2 = " + std::to_string(planes) +
-                                                  " interior planes exceed the static scratch of " +
-                                                  std::to_string(MCG_STATIC_SCRATCH_PLANES) + " planes");
-    const double n = double(NX) * NY * NZ;
-    if (n >= 2147483647.0) return mcg::fail(MCG_ERR_INVALID_ARG, "NX*NY*NZ must be < 2^31");
-    double *partials = nullptr;
-    if (mcg_status s = scratch_on_current_device(&partials)) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    k_plane_sums<<<planes, kThreads, 0, st>>>(fr, fb, NX, NY, size_t(n), partials);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return mcg::cuda_fail(e, "plane sums kernel");
-    k_fold_planes<<<1, kThreads, 0, st>>>(partials, planes, out5);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return mcg::cuda_fail(e, "fold kernel");
-    return MCG_OK;
+    return mcg::guarded([&]() -> mcg_status {
+        if (!fr || !fb || !out5) return mcg::fail(MCG_ERR_INVALID_ARG, "fr, fb and out5 must be device pointers");
+        if (NX < 3 || NY < 3 || NZ < 3) return mcg::fail(MCG_ERR_INVALID_ARG, "NX, NY, NZ must be >= 3");
+        const int planes = NZ - 2;
+        if (planes > MCG_STATIC_SCRATCH_PLANES)
+            return mcg::fail(MCG_ERR_INVALID_ARG, "NZ - 2 = " + std::to_string(planes) +
+                                                      " interior planes exceed the static scratch of " +
+                                                      std::to_string(MCG_STATIC_SCRATCH_PLANES) + " planes");
+        const double n = double(NX) * NY * NZ;
+        if (n >= 2147483647.0) return mcg::fail(MCG_ERR_INVALID_ARG, "NX*NY*NZ must be < 2^31");
+        double *partials = nullptr;
+        if (mcg_status s = scratch_on_current_device(&partials)) return s;
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        k_plane_sums<<<planes, kThreads, 0, st>>>(fr, fb, NX, NY, size_t(n), partials);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            k_fold_planes<<<1, kThreads, 0, st>>>(partials, planes, out5);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) {
+            forget_scratch_on_current_device();  // looked up again by the next call
+            return mcg::cuda_fail(e, "conservation sums kernels");
+        }
+        return MCG_OK;
+    });
 }

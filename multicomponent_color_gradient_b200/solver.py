@@ -222,9 +222,15 @@ class Solver:
                 arrs.append(a)
         self._c("mcg_set_fields", *[(_fptr(a) if a is not None else None) for a in arrs])
 
-    def get_fields(self) -> Dict[str, np.ndarray]:
-        out = {k: np.empty(self.N, np.float32) for k in ("rhor", "rhob", "ux", "uy", "uz")}
-        self._c("mcg_get_fields", *[_fptr(out[k]) for k in ("rhor", "rhob", "ux", "uy", "uz")])
+    def get_fields(self, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """rhor, rhob, ux, uy, uz of the current state; `out` may give the
+        destination arrays (float32, Ncells each, e.g. views of pinned memory)."""
+        keys = ("rhor", "rhob", "ux", "uy", "uz")
+        if out is None:
+            out = {k: np.empty(self.N, np.float32) for k in keys}
+        for k in keys:
+            assert out[k].dtype == np.float32 and out[k].size == self.N and out[k].flags.c_contiguous
+        self._c("mcg_get_fields", *[_fptr(out[k]) for k in keys])
         return out
 
     def get_stress(self) -> np.ndarray:

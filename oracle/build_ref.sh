@@ -18,6 +18,9 @@ if [ ! -f "$REF/kernels.cu" ]; then
     exit 0
 fi
 mkdir -p "$OUT"
+# where the sources were found, for tests that read the reference's post/
+# scripts in this checkout (oracle/_ref/ is a build folder, not committed)
+echo "$REF" > "$OUT/REFERENCE_DIR"
 PY="${PYTHON:-python}"
 CASES="${MCG_REF_CASES:-$("$PY" "$HERE/ref_constants.py" --list)}"
 for c in $CASES; do

@@ -34,3 +34,14 @@ def ref_binary(case: str):
     """Path of the reference's own CUDA build for a case, or None if not built."""
     p = os.path.join(ROOT, "oracle", "_ref", "ref_" + case)
     return p if os.path.exists(p) else None
+
+
+def reference_dir():
+    """The reference checkout: MCG_REFERENCE_DIR, else the directory
+    oracle/build_ref.sh compiled the reference from (recorded in
+    oracle/_ref/REFERENCE_DIR), when it exists on this machine; else None."""
+    d = os.environ.get("MCG_REFERENCE_DIR")
+    rec = os.path.join(ROOT, "oracle", "_ref", "REFERENCE_DIR")
+    if not d and os.path.exists(rec):
+        d = open(rec).read().strip()
+    return d if d and os.path.isdir(d) else None

@@ -72,8 +72,21 @@ def test_output_files_match_reference_layout(tmp_path):
             tke_o.append(O.total_tke())
             F = S.get_fields()
     S.write_radial_outputs()
-    for _ in range(3):
+    # uy_avg: the running mean of kernels.cu:168-186 over three different
+    # states (steps 61, 68, 75), restated in float32 numpy
+    m = np.zeros((NZ, NY, NX), bool)
+    m[1:-1, 1:-1, 1:-1] = True
+    m = m.ravel()
+    expect = np.zeros(N, np.float32)
+    samples_uy = []
+    for k in range(3):
+        if k:
+            S.step(7)
         S.launch_update_uy_average()
+        uy = S.get_fields()["uy"]
+        samples_uy.append(uy)
+        c = np.float32(k)
+        expect = np.where(m, (expect * c + uy) / (c + np.float32(1)), np.float32(0)).astype(np.float32)
     S.write_uy_average()
     case_dir, mean_dir, vti_dir = S.output_dirs()
     assert case_dir.endswith(os.path.join("JET_VTK", "Re45_We3"))
@@ -110,9 +123,12 @@ def test_output_files_match_reference_layout(tmp_path):
     # uy_avg.bin: float32 Ncells as post/binConversionVti.py:22-28 reads it
     uy_avg = np.fromfile(os.path.join(mean_dir, "uy_avg.bin"), np.float32)
     assert uy_avg.size == N
-    m = np.zeros((NZ, NY, NX), bool)
-    m[1:-1, 1:-1, 1:-1] = True
-    np.testing.assert_allclose(uy_avg[m.ravel()], F["uy"][m.ravel()], rtol=1e-5, atol=1e-7)
+    assert not np.any(uy_avg[~m])  # ghost nodes are not averaged
+    np.testing.assert_allclose(uy_avg[m], expect[m], rtol=1e-6, atol=1e-9)
+    # the three samples differ, so a wrong weighting would show: the mean is
+    # neither the last sample nor the first
+    for u in (samples_uy[0], samples_uy[-1]):
+        assert np.max(np.abs(uy_avg[m] - u[m])) > 100 * (1e-6 * np.max(np.abs(expect[m])) + 1e-9)
 
 
 @pytest.mark.parametrize("async_output", ["0", "1"])

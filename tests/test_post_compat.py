@@ -5,8 +5,8 @@ tests/golden/make_post_fixture.py on a GPU) read back
 * by the reference's own post/mean_profile_io.py (read_metadata,
   read_radial_moments, require_samples, averaged_radial_fields,
   fit_virtual_origin: post/mean_profile_io.py:61-239), imported from the
-  reference checkout that MCG_REFERENCE_ROOT names, when one is present,
-  else skipped;
+  reference checkout (MCG_REFERENCE_DIR, or the one oracle/build_ref.sh
+  compiled from), when one is present, else skipped;
 * by the package's plain-XML replacement of post/binConversionVti.py, which
   needs no vtk package.
 """
@@ -20,19 +20,21 @@ import sys
 import numpy as np
 import pytest
 
+from conftest import reference_dir
 from multicomponent_color_gradient_b200.post import read_case_info, write_uy_avg_vti
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASE_DIR = os.path.join(HERE, "golden", "post_jet_24x40x24", "JET_VTK", "Re45_We3")
 MEAN_DIR = os.path.join(CASE_DIR, "mean_profiles")
-REF_POST = os.path.join(os.environ.get("MCG_REFERENCE_ROOT", "/root/reference"), "post")
+REF_DIR = reference_dir()
+REF_POST = os.path.join(REF_DIR, "post") if REF_DIR else None
 NX, NY, NZ, NRB = 24, 40, 24, 12
 SAMPLES = 51  # statistics from step 10 to step 60
 
 
 @pytest.fixture(scope="module")
 def ref_post():
-    if not os.path.isfile(os.path.join(REF_POST, "mean_profile_io.py")):
+    if REF_POST is None or not os.path.isfile(os.path.join(REF_POST, "mean_profile_io.py")):
         pytest.skip("the reference's post/ scripts are not present")
     sys.path.insert(0, REF_POST)
     try:
