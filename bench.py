@@ -181,50 +181,87 @@ def cpu_baseline(case_name: str, seconds: float):
             "sample": f"{steps} steps of {case_name} (float64 OpenMP oracle, radial statistics on), {dt:.1f} s"}
 
 
-def adjoint_cost(steps: int):
-    """Discrete-adjoint cost on the 96^3 periodic bubble (R=20, tau 0.7, sigma
-    0.01): device time of one forward + reverse sweep over `steps` steps (a
-    moment record per state) against `steps` plain forward steps."""
+def adjoint_cost(steps: int, snapshots: int):
+    """The bubble adjoint at its configuration: 96^3 periodic box, R = 20, tau
+    0.7, sigma 0.01; initial velocity a seeded sum of divergence-free Fourier
+    modes with wave numbers up to 8 per axis (4912 amplitudes) scaled to a
+    peak of 0.01; J = sum (psi_T - psi*)^2 against psi* of a run with sigma =
+    0.012 from the same state; `snapshots` held states (binomial
+    checkpointing).  Device time of one forward + reverse sweep against
+    `steps` plain forward steps."""
     import numpy as np
 
     from multicomponent_color_gradient_b200.adjoint import BubbleProblem
 
-    P = BubbleProblem("adjoint_bubble_96", nsteps=steps, max_mode=1, seed=1, relax_steps=0)
+    P = BubbleProblem("adjoint_bubble_96", nsteps=steps, snapshots=snapshots, max_mode=8, seed=1, relax_steps=50)
     try:
-        a = np.random.default_rng(2).normal(scale=2e-3, size=P.modes.count)
-        P.evaluate(a)
+        a = np.random.default_rng(2).normal(size=P.modes.count)
+        a *= 0.01 / np.abs(P.modes.velocity(a)).max()
+        u = P.initial_velocity(a)
+        T = P.solver(0.012, P.case["taub"])
+        T.init_equilibrium(P.rhor, P.rhob, u[0], u[1], u[2])
+        T.step(steps)
+        fr, fb = T.get_populations()
+        rr, rb = fr.reshape(27, -1).sum(0, dtype=np.float64), fb.reshape(27, -1).sum(0, dtype=np.float64)
+        P.target = ((rr - rb) / (rr + rb)).astype(np.float32)
+        P.evaluate(a)  # warm-up
         r = P.evaluate(a)
         S = P.solver(P.case["sigma"], P.case["taub"])
-        u = P.initial_velocity(a)
         S.init_equilibrium(P.rhor, P.rhob, u[0], u[1], u[2])
         S.step(3)
         fwd = S.step_timed(steps)
         return {"value": round(r["ms"] / fwd, 3), "unit": "adjoint sweep / forward run", "workload": "adjoint_bubble_96",
-                "steps": steps, "sweep_ms": round(r["ms"], 3), "forward_ms": round(fwd, 3),
-                "forward_steps_in_sweep": r["forward_steps"]}
+                "steps": steps, "snapshots": snapshots, "sweep_ms": round(r["ms"], 3), "forward_ms": round(fwd, 3),
+                "forward_steps_in_sweep": r["forward_steps"], "J": r["J"], "dJ_dsigma": r["dJ_dsigma"],
+                "dJ_dtau": r["dJ_dtau"], "amplitudes": int(P.modes.count),
+                "objective": "sum (psi_T - psi*)^2, psi* from sigma = 0.012"}
     finally:
         P.close()
 
 
-def jet_adjoint_cost(steps: int, segment: int):
-    """Jet adjoint cost on the bench jet (128x256x128): one forward + reverse
-    sweep over `steps` steps (objective over the second half, y >= 64, inlet
-    profile gradient) against `steps` plain forward steps."""
+def jet_adjoint_cost(steps: int, segment: int, storage: str):
+    """The jet adjoint at its configuration: jet 128x256x128, inlet profile of
+    8 Bessel coefficients seeded around the top-hat (N(0, 0.02)), T = `steps`,
+    J = the misfit of the time-averaged centreline velocity and half-width over
+    the second half of the run for 2 <= y/D <= 10, against the profiles of a
+    run with the coefficients perturbed by N(0, 0.05); forward states stored in
+    `storage`, float32 adjoint, a snapshot every `segment` steps.  Device time
+    of one sweep against `steps` plain forward steps of the same storage (and
+    of float32 storage)."""
     import numpy as np
 
     from multicomponent_color_gradient_b200 import Solver, get_case
 
-    with Solver(get_case(DEFAULT_CASE, NSTATS_START_STEP=10 ** 9)) as S:
-        S.set_inlet_bessel(np.zeros(8, np.float32))
+    rng = np.random.default_rng(5)
+    c0 = rng.normal(scale=0.02, size=8).astype(np.float32)
+    ct = (c0 + rng.normal(scale=0.05, size=8)).astype(np.float32)
+    t_begin, t_end = steps // 2, steps - 1
+    case = get_case(DEFAULT_CASE, storage=storage, NSTATS_START_STEP=t_begin)
+    D = 2 * int(case["jet_radius"])
+    y_lo, y_hi = 2 * D, min(10 * D, case["NY"] - 2)
+    with Solver(case) as S:
+        S.set_inlet_bessel(ct)
         S.init_jet()
-        S.adjoint_jet_run(20, 10, 19, 64)  # warm-up
-        r = S.adjoint_jet_run(steps, steps // 2, steps - 1, 64, segment=segment)
+        S.step(t_end + 1)
+        uc_t, rh_t = S.jet_profile_metrics()
+        S.set_inlet_bessel(c0)
+        S.init_jet()
+        r = S.adjoint_jet_profile_run(steps, t_begin, t_end, y_lo, y_hi, uc_t, rh_t, segment=segment)
         S.init_jet()
         S.step(3)
         fwd = S.step_timed(steps)
+    with Solver(get_case(DEFAULT_CASE, NSTATS_START_STEP=10 ** 9)) as S32:
+        S32.init_jet()
+        S32.step(3)
+        fwd32 = S32.step_timed(steps)
     return {"value": round(r["ms"] / fwd, 3), "unit": "adjoint sweep / forward run", "workload": DEFAULT_CASE,
-            "steps": steps, "segment": segment, "sweep_ms": round(r["ms"], 3), "forward_ms": round(fwd, 3),
-            "forward_steps_in_sweep": r["forward_steps"], "gradient": "inlet-profile Bessel coefficients"}
+            "storage": storage, "steps": steps, "segment": segment, "sweep_ms": round(r["ms"], 3),
+            "forward_ms": round(fwd, 3), "vs_float32_forward": round(r["ms"] / fwd32, 3),
+            "forward_ms_float32": round(fwd32, 3), "forward_steps_in_sweep": r["forward_steps"], "J": r["J"],
+            "dJ_dc": [round(float(v), 9) for v in r["dJ_dc"]],
+            "objective": f"time-averaged centreline uy and half-width misfit, steps {t_begin}..{t_end}, "
+                         f"y {y_lo}..{y_hi}",
+            "gradient": "inlet-profile Bessel coefficients"}
 
 
 def run_reference(args, world, rank):
@@ -279,9 +316,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost measurement")
-    ap.add_argument("--adjoint-steps", type=int, default=100)
-    ap.add_argument("--jet-adjoint-steps", type=int, default=400, help="steps of the jet-adjoint cost measurement")
-    ap.add_argument("--jet-adjoint-segment", type=int, default=100, help="checkpoint segment of the jet adjoint")
+    ap.add_argument("--adjoint-steps", type=int, default=400, help="steps of the bubble adjoint (96^3)")
+    ap.add_argument("--adjoint-snapshots", type=int, default=20, help="held states of the bubble adjoint")
+    ap.add_argument("--jet-adjoint-steps", type=int, default=4000, help="steps of the jet adjoint (128x256x128)")
+    ap.add_argument("--jet-adjoint-segment", type=int, default=200, help="checkpoint segment of the jet adjoint")
+    ap.add_argument("--jet-adjoint-storage", default="f16", choices=["f32", "f16"],
+                    help="storage of the jet adjoint's forward states")
     ap.add_argument("--shape", default=None,
                     help="NXxNYxNZ override of the case grid (smaller profiling captures); not a bench line")
     args = ap.parse_args()
@@ -442,11 +482,12 @@ def main():
     adjoint = jet_adjoint = None
     if not args.no_adjoint:
         try:
-            adjoint = adjoint_cost(args.adjoint_steps)
+            adjoint = adjoint_cost(args.adjoint_steps, args.adjoint_snapshots)
         except Exception as exc:
             adjoint = {"value": None, "error": str(exc)[:200]}
         try:
-            jet_adjoint = jet_adjoint_cost(args.jet_adjoint_steps, args.jet_adjoint_segment)
+            jet_adjoint = jet_adjoint_cost(args.jet_adjoint_steps, args.jet_adjoint_segment,
+                                           args.jet_adjoint_storage)
         except Exception as exc:
             jet_adjoint = {"value": None, "error": str(exc)[:200]}
 

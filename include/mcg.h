@@ -291,8 +291,8 @@ mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *r
 mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nsteps, int32_t snapshots,
                            double *J, double *dJ_dsigma, double *dJ_dtau, float *dJ_du0,
                            int64_t *forward_steps, float *ms);
-/* Discrete adjoint of nsteps steps of the jet (MCG_BOUNDARY_JET, float32
- * storage) from the handle's current state, boundary conditions included: the
+/* Discrete adjoint of nsteps steps of the jet (MCG_BOUNDARY_JET) from the
+ * handle's current state, boundary conditions included: the
  * inlet (jet/boundary_conditions.cuh:17-85) with its radial profile
  * (mcg_set_inlet_bessel) and the convective outlet with its carried state
  * (:163-233).  J = sum over steps t in [t_begin, t_end] of (1/2) sum of uy^2
@@ -304,9 +304,31 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
  * 48 B per node and step) and runs nsteps forward steps; with 0 < segment <
  * nsteps it keeps a snapshot (populations and outlet state, 216 B per node)
  * every `segment` steps and the tape of one segment, and runs about
- * 2*nsteps forward steps.  The handle's state is left as it was. */
+ * 2*nsteps forward steps.  The forward states keep the handle's storage: with
+ * MCG_STORAGE_F16 the sweep is the float32 adjoint of the step taken at the
+ * float16-stored forward states (snapshots then take 108 B per node).  The
+ * handle's state is left as it was. */
 mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
                                int32_t segment, double *J, double *dJ_dc, int64_t *forward_steps, float *ms);
+/* No counterpart in the reference.  The jet adjoint of mcg_adjoint_jet_run
+ * for a misfit of time-averaged profiles: over the window steps t_begin..t_end
+ * the radial statistics give the mean profile U(y, r) (the accumulation of
+ * kernels.cu:188-233, averaged as post/mean_profile_io.py:182-212 does), its
+ * centreline uc(y) = U(y, 0) and half-width r_half(y)
+ * (post/plot_profiles.py:53-91), and
+ *   J = 1/2 sum_{y_lo <= y <= y_hi} ((uc - uc_target)/U_jet)^2
+ *                                  + ((r_half - rhalf_target)/D)^2,
+ * each term where both of its values are defined (a NaN target drops it).
+ * uc_target, rhalf_target: [NY] (mcg_jet_profile_metrics of a target run).
+ * The sweep first runs the window forward for the averages, then reverses as
+ * mcg_adjoint_jet_run does (about nsteps more forward steps with segments). */
+mcg_status mcg_adjoint_jet_profile_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_lo,
+                                       int32_t y_hi, const float *uc_target, const float *rhalf_target, int32_t segment,
+                                       double *J, double *dJ_dc, int64_t *forward_steps, float *ms);
+/* No counterpart in the reference (post/plot_profiles.py forms the same
+ * quantities from the files).  Centreline velocity uc[NY] and half-width
+ * r_half[NY] (NaN where undefined) of the handle's radial statistics so far. */
+mcg_status mcg_jet_profile_metrics(mcg_handle *h, float *uc, float *r_half);
 /* The treeverse schedule without running it (host only, no device needed):
  * fused steps a reverse sweep over nsteps steps with `snapshots` held states
  * runs, and the recomputation depth r (least r with C(s + r, s) >= nsteps + 1,

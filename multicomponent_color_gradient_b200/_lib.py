@@ -96,6 +96,9 @@ SIGNATURES = {
     "mcg_adjoint_plan": [C.c_int32, C.c_int32, C.POINTER(C.c_int64), _I32],
     "mcg_adjoint_jet_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.POINTER(C.c_int64),
                             _F],
+    "mcg_adjoint_jet_profile_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _F, _F, C.c_int32, _D,
+                                    _D, C.POINTER(C.c_int64), _F],
+    "mcg_jet_profile_metrics": [_P, _F, _F],
     "mcg_output_open": [_P, C.c_char_p],
     "mcg_output_step": [_P, C.c_int32],
     "mcg_output_step_async": [_P, C.c_int32],

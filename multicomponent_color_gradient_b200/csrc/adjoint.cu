@@ -109,8 +109,11 @@ int64_t forward_steps_of(const std::vector<Action> &acts) {
     } while (0)
 
 struct DeviceBuffers {
+    cudaStream_t stream;  // the run's stream: buffers are cleared in its order
     std::vector<void *> ptrs;
+    explicit DeviceBuffers(cudaStream_t st) : stream(st) {}
     ~DeviceBuffers() {
+        if (!ptrs.empty()) cudaStreamSynchronize(stream);
         for (void *p : ptrs) cudaFree(p);
     }
     cudaError_t alloc(void **p, size_t bytes) {
@@ -118,7 +121,7 @@ struct DeviceBuffers {
         cudaError_t e = cudaMalloc(p, bytes);
         if (e != cudaSuccess) return e;
         ptrs.push_back(*p);
-        return cudaMemsetAsync(*p, 0, bytes);
+        return cudaMemsetAsync(*p, 0, bytes, stream);
     }
 };
 
@@ -249,7 +252,7 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
         std::vector<Action> acts;
         if (!tape_mode) plan(acts, 0, int64_t(nsteps) + 1, 0, free_slots);
 
-        DeviceBuffers buf;
+        DeviceBuffers buf(h->stream);
         Run run;
         run.h = h;
         run.base = h->s;
@@ -347,163 +350,251 @@ std::vector<float> bessel_basis(const mcg_params &p) {
 }
 }  // namespace
 
+namespace {
+// The objective of a jet adjoint run.  kind 0: J = sum over window steps of
+// (1/2) sum uy^2 over interior nodes with y >= y_obs.  kind 1: the misfit of
+// the window's time-averaged centreline velocity and half-width (see
+// mcg_adjoint_jet_profile_run) against targets for y in [y_lo, y_hi].
+struct JetObjective {
+    int kind = 0;
+    int y_obs = 0;
+    int y_lo = 0, y_hi = -1;
+    const float *uc_target = nullptr, *rh_target = nullptr;
+};
+
+mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t segment,
+                       const JetObjective &objective, double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
+    if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+    if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
+    if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
+        return fail(MCG_ERR_INVALID_ARG, "need 0 <= t_begin <= t_end < nsteps");
+    if (h->p.boundary != MCG_BOUNDARY_JET) return fail(MCG_ERR_UNSUPPORTED, "the jet adjoint covers the jet boundary");
+    if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
+    if (mcg_status st = mcg::async_flush(h)) return st;
+    const mcg::Geometry &g = h->s.g;
+    const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
+    const size_t NRB = size_t(g.NX / 2), M = size_t(g.NY) * NRB;
+    // the forward states keep the handle's storage (float16 or float32); the
+    // reverse sweep reads them only through their float32 moment records, and
+    // its lambda arrays are float32 pairs
+    const size_t state_bytes = g.storage == MCG_STORAGE_F16 ? size_t(mcg::kQ) * N * 4 : size_t(2 * mcg::kQ) * N * 4;
+    const size_t lam_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);
+    const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
+    const int nb = mcg::kInletBesselMax;
+    const bool profile = objective.kind == 1;
+
+    DeviceBuffers buf(h->stream);
+    void *p = nullptr;
+    mcg::DeviceState run = h->s;
+    void *work[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, state_bytes), "jet adjoint work buffers");
+        work[k] = p;
+    }
+    // both buffers: slots no kernel rewrites carry their initial values in both
+    ADJ_CUDA(cudaMemcpyAsync(work[0], h->s.pops[h->cur], state_bytes, cudaMemcpyDeviceToDevice, h->stream),
+             "copy state");
+    ADJ_CUDA(cudaMemcpyAsync(work[1], h->s.pops[h->cur ^ 1], state_bytes, cudaMemcpyDeviceToDevice, h->stream),
+             "copy state");
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment planes");
+    run.mom = static_cast<float *>(p);
+    ADJ_CUDA(cudaMemcpyAsync(run.mom, h->s.mom, size_t(mcg::kMomCount) * N * sizeof(float), cudaMemcpyDeviceToDevice,
+                             h->stream),
+             "copy moments");
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "jet adjoint psi planes");
+        run.psi[k] = static_cast<float *>(p);
+        ADJ_CUDA(cudaMemcpyAsync(run.psi[k], h->s.psi[k], N * sizeof(float), cudaMemcpyDeviceToDevice, h->stream),
+                 "copy psi");
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
+    run.bmom = static_cast<float *>(p);
+    // the run's own radial sums (the profile objective's time averages)
+    ADJ_CUDA(buf.alloc(&p, 5 * M * sizeof(double)), "jet adjoint radial sums");
+    run.radial = static_cast<double *>(p);
+    // segments of L steps: a snapshot (populations + outlet state) at the
+    // start of each, and a tape of one segment's records
+    const int64_t L = (segment <= 0 || segment >= nsteps) ? nsteps : segment;
+    const int64_t nseg = (nsteps + L - 1) / L;
+    std::vector<void *> snap(size_t(nseg), nullptr);
+    std::vector<float *> snapB(size_t(nseg), nullptr);
+    for (int64_t j = 0; j < nseg; ++j) {
+        ADJ_CUDA(buf.alloc(&p, state_bytes), "jet adjoint snapshots");
+        snap[size_t(j)] = p;
+        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
+        snapB[size_t(j)] = static_cast<float *>(p);
+    }
+    float *tape = nullptr;
+    ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
+    tape = static_cast<float *>(p);
+    float *lam[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, lam_bytes), "jet adjoint lambda buffers");
+        lam[k] = static_cast<float *>(p);
+    }
+    ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment adjoints");
+    float *lmom = static_cast<float *>(p);
+    ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "jet adjoint gradient adjoints");
+    float *lf = static_cast<float *>(p);
+    float *LB[2];
+    for (int k = 0; k < 2; ++k) {
+        ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint outlet adjoints");
+        LB[k] = static_cast<float *>(p);
+    }
+    const std::vector<float> basis = bessel_basis(h->p);
+    ADJ_CUDA(buf.alloc(&p, basis.size() * sizeof(float)), "jet adjoint profile basis");
+    float *dbasis = static_cast<float *>(p);
+    ADJ_CUDA(cudaMemcpyAsync(dbasis, basis.data(), basis.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+             "upload profile basis");
+    ADJ_CUDA(buf.alloc(&p, (2 + size_t(nb)) * sizeof(double)), "jet adjoint accumulators");
+    double *acc = static_cast<double *>(p);  // [0] J, [1] (unused), [2..] dJ/dc_k
+    double *dacc_w = nullptr;
+    ADJ_CUDA(buf.alloc(&p, 2 * sizeof(double)), "jet adjoint parameter partials");
+    dacc_w = static_cast<double *>(p);
+    float *table = nullptr;
+    if (profile) {
+        ADJ_CUDA(buf.alloc(&p, M * sizeof(float)), "jet adjoint profile source");
+        table = static_cast<float *>(p);
+    }
+
+    const int64_t step0 = h->step;
+    ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
+    int64_t fwd = 0;
+    // one forward step t of the run's state (work[t & 1] -> work[(t+1) & 1]),
+    // recording into `rec` when given: its psi with the ghost values it reads,
+    // the outlet state before its boundary, and (the fused step) its moments;
+    // `stats` adds the step's radial statistics to the run's sums
+    auto forward = [&](int64_t t, float *rec, bool stats) -> mcg_status {
+        mcg::DeviceState d = run;
+        d.pops[0] = work[t & 1];
+        d.pops[1] = work[(t + 1) & 1];
+        if (rec) {
+            ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, h->stream),
+                     "record psi");
+            ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
+                       "jet adjoint: record outlet state");
+            d.tape = rec;
+        }
+        ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, stats, h->stream), "jet adjoint: forward step");
+        d.tape = nullptr;
+        ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
+        ++fwd;
+        return MCG_OK;
+    };
+    auto save = [&](int64_t j, int64_t t) -> mcg_status {
+        ADJ_CUDA(cudaMemcpyAsync(snap[size_t(j)], work[t & 1], state_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                 "save snapshot");
+        ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(run, snapB[size_t(j)], h->stream), "jet adjoint: save outlet");
+        return MCG_OK;
+    };
+    // ---- pass 1: snapshots at every segment start; the profile objective runs
+    // at least through the window here, accumulating its radial statistics
+    if (mcg_status st = save(0, 0)) return st;
+    const int64_t pass1 = profile ? std::max<int64_t>(int64_t(t_end) + 1, (nseg - 1) * L) : (nseg - 1) * L;
+    for (int64_t t = 0; t < pass1; ++t) {
+        if (mcg_status st = forward(t, nullptr, profile && t >= t_begin && t <= t_end)) return st;
+        if ((t + 1) % L == 0 && (t + 1) / L < nseg)
+            if (mcg_status st = save((t + 1) / L, t + 1)) return st;
+    }
+    double J_host = 0.0;
+    if (profile) {
+        // J and its source dJ/duy per (y, radial bin) from the window's averages
+        std::vector<double> sum_uy(M);
+        ADJ_CUDA(cudaMemcpyAsync(sum_uy.data(), run.radial, M * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                 "download radial sums");
+        ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint forward pass");
+        const uint32_t samples = uint32_t(t_end - t_begin + 1);
+        std::vector<float> src(M, 0.0f);
+        J_host = mcg::profile_objective(h, sum_uy.data(), samples, objective.y_lo, objective.y_hi, objective.uc_target,
+                                        objective.rh_target, src.data());
+        ADJ_CUDA(cudaMemcpyAsync(table, src.data(), M * sizeof(float), cudaMemcpyHostToDevice, h->stream),
+                 "upload profile source");
+        ADJ_CUDA(cudaStreamSynchronize(h->stream), "upload profile source");
+    }
+    // ---- pass 2: per segment from the last, restore, re-run recording, reverse
+    int lc = 0, lb = 0;
+    for (int64_t j = nseg - 1; j >= 0; --j) {
+        const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
+        ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], state_bytes, cudaMemcpyDeviceToDevice, h->stream),
+                 "restore snapshot");
+        ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
+                   "jet adjoint: restore outlet");
+        for (int64_t t = s0; t < s1; ++t)
+            if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats, false)) return st;
+        for (int64_t t = s1 - 1; t >= s0; --t) {
+            const float *rec = tape + size_t(t - s0) * rec_floats;
+            const bool in_window = t >= t_begin && t <= t_end;
+            mcg::AdjObjective obj{in_window && !profile ? 1.0f : 0.0f, objective.y_obs, profile ? nullptr : acc};
+            if (profile && in_window) obj.table = table;
+            ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
+                       "jet adjoint: collision");
+            ADJ_LAUNCH(h,
+                       mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
+                                                lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
+                       "jet adjoint: boundary");
+            ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream), "jet adjoint: moments");
+            lc ^= 1;
+            lb ^= 1;
+        }
+    }
+    ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
+    std::vector<double> out(2 + size_t(nb));
+    ADJ_CUDA(cudaMemcpyAsync(out.data(), acc, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+             "download J");
+    ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint run");
+    float t_ms = 0.f;
+    ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
+    if (J) *J = profile ? J_host : out[0];
+    if (dJ_dc)
+        for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
+    if (forward_steps) *forward_steps = fwd;
+    if (ms) *ms = t_ms;
+    return MCG_OK;
+}
+}  // namespace
+
 mcg_status mcg_adjoint_jet_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_obs,
                                int32_t segment, double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
     return mcg::guarded([&]() -> mcg_status {
+        JetObjective obj;
+        obj.kind = 0;
+        obj.y_obs = y_obs;
+        return jet_adjoint(h, nsteps, t_begin, t_end, segment, obj, J, dJ_dc, forward_steps, ms);
+    });
+}
+
+mcg_status mcg_adjoint_jet_profile_run(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t_end, int32_t y_lo,
+                                       int32_t y_hi, const float *uc_target, const float *rhalf_target, int32_t segment,
+                                       double *J, double *dJ_dc, int64_t *forward_steps, float *ms) {
+    return mcg::guarded([&]() -> mcg_status {
         if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
-        if (nsteps < 1) return fail(MCG_ERR_INVALID_ARG, "nsteps must be >= 1");
-        if (t_begin < 0 || t_end < t_begin || t_end >= nsteps)
-            return fail(MCG_ERR_INVALID_ARG, "need 0 <= t_begin <= t_end < nsteps");
-        if (h->p.boundary != MCG_BOUNDARY_JET || h->p.storage != MCG_STORAGE_F32)
-            return fail(MCG_ERR_UNSUPPORTED, "the jet adjoint covers the jet boundary with float32 storage");
-        if (h->p.sponge_K != 0.0f) return fail(MCG_ERR_UNSUPPORTED, "the adjoint needs a uniform relaxation rate");
-        const mcg::Geometry &g = h->s.g;
-        const size_t N = g.N, NP = size_t(g.NX) * g.NZ;
-        const size_t pop_bytes = size_t(2 * mcg::kQ) * N * sizeof(float);  // float32 populations or lambda
-        const size_t rec_floats = size_t(mcg::kTapePlanes) * N + 5 * NP;  // moments, psi with ghosts, outlet state
-        const int nb = mcg::kInletBesselMax;
+        if (!uc_target || !rhalf_target) return fail(MCG_ERR_INVALID_ARG, "target profiles must not be null");
+        if (y_lo < 1 || y_hi > h->p.NY - 2 || y_hi < y_lo)
+            return fail(MCG_ERR_INVALID_ARG, "need 1 <= y_lo <= y_hi <= NY-2");
+        JetObjective obj;
+        obj.kind = 1;
+        obj.y_lo = y_lo;
+        obj.y_hi = y_hi;
+        obj.uc_target = uc_target;
+        obj.rh_target = rhalf_target;
+        return jet_adjoint(h, nsteps, t_begin, t_end, segment, obj, J, dJ_dc, forward_steps, ms);
+    });
+}
 
-        DeviceBuffers buf;
-        void *p = nullptr;
-        mcg::DeviceState run = h->s;
-        void *work[2];
-        for (int k = 0; k < 2; ++k) {
-            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint work buffers");
-            work[k] = p;
-        }
-        // both buffers: slots no kernel rewrites carry their initial values in both
-        ADJ_CUDA(cudaMemcpyAsync(work[0], h->s.pops[h->cur], pop_bytes, cudaMemcpyDeviceToDevice, h->stream), "copy state");
-        ADJ_CUDA(cudaMemcpyAsync(work[1], h->s.pops[h->cur ^ 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                 "copy state");
-        ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment planes");
-        run.mom = static_cast<float *>(p);
-        ADJ_CUDA(cudaMemcpyAsync(run.mom, h->s.mom, size_t(mcg::kMomCount) * N * sizeof(float), cudaMemcpyDeviceToDevice,
-                                 h->stream),
-                 "copy moments");
-        for (int k = 0; k < 2; ++k) {
-            ADJ_CUDA(buf.alloc(&p, N * sizeof(float)), "jet adjoint psi planes");
-            run.psi[k] = static_cast<float *>(p);
-            ADJ_CUDA(cudaMemcpyAsync(run.psi[k], h->s.psi[k], N * sizeof(float), cudaMemcpyDeviceToDevice, h->stream),
-                     "copy psi");
-        }
-        ADJ_CUDA(buf.alloc(&p, size_t(2) * g.NZ * mcg::kMomCount * g.NX * sizeof(float)), "jet adjoint bmom");
-        run.bmom = static_cast<float *>(p);
-        // segments of L steps: a snapshot (populations + outlet state) at the
-        // start of each, and a tape of one segment's records
-        const int64_t L = (segment <= 0 || segment >= nsteps) ? nsteps : segment;
-        const int64_t nseg = (nsteps + L - 1) / L;
-        std::vector<void *> snap(size_t(nseg), nullptr);
-        std::vector<float *> snapB(size_t(nseg), nullptr);
-        for (int64_t j = 0; j < nseg; ++j) {
-            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint snapshots");
-            snap[size_t(j)] = p;
-            ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
-            snapB[size_t(j)] = static_cast<float *>(p);
-        }
-        float *tape = nullptr;
-        ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
-        tape = static_cast<float *>(p);
-        float *lam[2];
-        for (int k = 0; k < 2; ++k) {
-            ADJ_CUDA(buf.alloc(&p, pop_bytes), "jet adjoint lambda buffers");
-            lam[k] = static_cast<float *>(p);
-        }
-        ADJ_CUDA(buf.alloc(&p, size_t(mcg::kMomCount) * N * sizeof(float)), "jet adjoint moment adjoints");
-        float *lmom = static_cast<float *>(p);
-        ADJ_CUDA(buf.alloc(&p, 3 * N * sizeof(float)), "jet adjoint gradient adjoints");
-        float *lf = static_cast<float *>(p);
-        float *LB[2];
-        for (int k = 0; k < 2; ++k) {
-            ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint outlet adjoints");
-            LB[k] = static_cast<float *>(p);
-        }
-        const std::vector<float> basis = bessel_basis(h->p);
-        ADJ_CUDA(buf.alloc(&p, basis.size() * sizeof(float)), "jet adjoint profile basis");
-        float *dbasis = static_cast<float *>(p);
-        ADJ_CUDA(cudaMemcpyAsync(dbasis, basis.data(), basis.size() * sizeof(float), cudaMemcpyHostToDevice, h->stream),
-                 "upload profile basis");
-        ADJ_CUDA(buf.alloc(&p, (2 + size_t(nb)) * sizeof(double)), "jet adjoint accumulators");
-        double *acc = static_cast<double *>(p);  // [0] J, [1] (unused), [2..] dJ/dc_k
-        double *dacc_w = nullptr;
-        ADJ_CUDA(buf.alloc(&p, 2 * sizeof(double)), "jet adjoint parameter partials");
-        dacc_w = static_cast<double *>(p);
-
-        const int64_t step0 = h->step;
-        ADJ_CUDA(cudaEventRecord(h->ev0, h->stream), "event");
-        int64_t fwd = 0;
-        // one forward step t of the run's state (work[t & 1] -> work[(t+1) & 1]),
-        // recording into `rec` when given: its psi with the ghost values it reads,
-        // the outlet state before its boundary, and (k_fused) its moments
-        auto forward = [&](int64_t t, float *rec) -> mcg_status {
-            mcg::DeviceState d = run;
-            d.pops[0] = work[t & 1];
-            d.pops[1] = work[(t + 1) & 1];
-            if (rec) {
-                ADJ_CUDA(cudaMemcpyAsync(rec + size_t(mcg::kTapePsi) * N, run.psi[(step0 + t) & 1], N * sizeof(float),
-                                         cudaMemcpyDeviceToDevice, h->stream),
-                         "record psi");
-                ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(d, rec + size_t(mcg::kTapePlanes) * N, h->stream),
-                           "jet adjoint: record outlet state");
-                d.tape = rec;
-            }
-            ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, false, h->stream), "jet adjoint: forward step");
-            d.tape = nullptr;
-            ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
-            ++fwd;
-            return MCG_OK;
-        };
-        auto save = [&](int64_t j, int64_t t) -> mcg_status {
-            ADJ_CUDA(cudaMemcpyAsync(snap[size_t(j)], work[t & 1], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                     "save snapshot");
-            ADJ_LAUNCH(h, mcg::launch_copy_outlet_state(run, snapB[size_t(j)], h->stream), "jet adjoint: save outlet");
-            return MCG_OK;
-        };
-        // ---- pass 1 (several segments only): snapshots at every segment start
-        if (mcg_status st = save(0, 0)) return st;
-        if (nseg > 1)
-            for (int64_t t = 0; t < (nseg - 1) * L; ++t) {
-                if (mcg_status st = forward(t, nullptr)) return st;
-                if ((t + 1) % L == 0)
-                    if (mcg_status st = save((t + 1) / L, t + 1)) return st;
-            }
-        // ---- pass 2: per segment from the last, restore, re-run recording, reverse
-        int lc = 0, lb = 0;
-        for (int64_t j = nseg - 1; j >= 0; --j) {
-            const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
-            ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], pop_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                     "restore snapshot");
-            ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
-                       "jet adjoint: restore outlet");
-            for (int64_t t = s0; t < s1; ++t)
-                if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats)) return st;
-            for (int64_t t = s1 - 1; t >= s0; --t) {
-                const float *rec = tape + size_t(t - s0) * rec_floats;
-                const bool in_window = t >= t_begin && t <= t_end;
-                const mcg::AdjObjective obj{in_window ? 1.0f : 0.0f, y_obs, acc};
-                ADJ_LAUNCH(h, mcg::launch_adj_collide(run, rec, lam[lc], lmom, lf, dacc_w, obj, h->stream),
-                           "jet adjoint: collision");
-                ADJ_LAUNCH(h,
-                           mcg::launch_adj_boundary(run, step0 + t, rec, rec + size_t(mcg::kTapePlanes) * N, lam[lc], lf,
-                                                    lmom, LB[lb], LB[lb ^ 1], dbasis, nb, acc + 2, h->stream),
-                           "jet adjoint: boundary");
-                ADJ_LAUNCH(h, mcg::launch_adj_moments(run, rec, lmom, lf, lam[lc ^ 1], h->stream),
-                           "jet adjoint: moments");
-                lc ^= 1;
-                lb ^= 1;
-            }
-        }
-        ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
-        std::vector<double> out(2 + size_t(nb));
-        ADJ_CUDA(cudaMemcpyAsync(out.data(), acc, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
-                 "download J");
-        ADJ_CUDA(cudaStreamSynchronize(h->stream), "jet adjoint run");
-        float t_ms = 0.f;
-        ADJ_CUDA(cudaEventElapsedTime(&t_ms, h->ev0, h->ev1), "event time");
-        if (J) *J = out[0];
-        if (dJ_dc)
-            for (int k = 0; k < nb; ++k) dJ_dc[k] = out[2 + size_t(k)];
-        if (forward_steps) *forward_steps = fwd;
-        if (ms) *ms = t_ms;
+mcg_status mcg_jet_profile_metrics(mcg_handle *h, float *uc, float *r_half) {
+    return mcg::guarded([&]() -> mcg_status {
+        if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+        if (!uc || !r_half) return fail(MCG_ERR_INVALID_ARG, "output arrays must not be null");
+        if (mcg_status st = mcg::async_flush(h)) return st;
+        if (!h->stats_started || h->stats_samples == 0)
+            return fail(MCG_ERR_STATE, "no radial statistics have been accumulated");
+        const size_t M = size_t(h->p.NY) * size_t(h->p.NX / 2);
+        std::vector<double> sum_uy(M);
+        ADJ_CUDA(cudaMemcpyAsync(sum_uy.data(), h->s.radial, M * sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+                 "download radial sums");
+        ADJ_CUDA(cudaStreamSynchronize(h->stream), "profile metrics");
+        mcg::profile_metrics(h, sum_uy.data(), h->stats_samples, uc, r_half);
         return MCG_OK;
     });
 }

@@ -110,6 +110,16 @@ mcg_status io_write_radial_host(mcg_handle *h, const StatsSnapshot &st, const do
 // text: the four base64 arrays laid out by vti_text_layout (launch_vti_encode).
 mcg_status io_write_vti_text(mcg_handle *h, const std::string &path, const char *text);
 mcg_status io_write_tke_sample_snap(mcg_handle *h, int32_t step, const StatsSnapshot &st);
+// Time-averaged jet profiles (profile.cpp), from the radial sums of uy
+// (sum_uy [NY*NR_BINS], `samples` steps): the centreline velocity uc[y] (bin 0)
+// and the half-width rh[y] (NaN where undefined), as the reference's
+// post/plot_profiles.py:53-91 forms them.
+void profile_metrics(const mcg_handle *h, const double *sum_uy, uint32_t samples, float *uc, float *rh);
+// J = 1/2 sum_{y_lo<=y<=y_hi} ((uc - uc*)/U)^2 + ((rh - rh*)/D)^2 over the y
+// where every value is defined, and src[y*NR_BINS + r] = dJ/duy of one node
+// of bin r at one window step (dJ/d(mean) / (samples * columns of the bin)).
+double profile_objective(const mcg_handle *h, const double *sum_uy, uint32_t samples, int y_lo, int y_hi,
+                         const float *uc_target, const float *rh_target, float *src);
 // Asynchronous outputs (output_async.cpp): wait for pending writes; release.
 mcg_status async_flush(mcg_handle *h);
 mcg_status async_enqueue(mcg_handle *h, int32_t step);

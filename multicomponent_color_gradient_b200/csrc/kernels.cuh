@@ -172,10 +172,15 @@ cudaError_t launch_check_finite(const DeviceState &s, int cur, int *flag, cudaSt
 
 // Objective source of an adjoint step: J_t = (weight/2) sum of uy^2 over
 // interior nodes with y >= y_obs (weight 0: none); J accumulates J_t (or null).
+// With `table` ([NY][NRB]) the source instead is dJ/duy = table[y][rb] at the
+// nodes of radial bin rb < NRB (the bins of the radial statistics), the
+// adjoint of an objective of the time-averaged radial profiles of uy; J is
+// then formed on the host.
 struct AdjObjective {
     float weight;
     int y_obs;
     double *J;
+    const float *table = nullptr;
 };
 
 // ---- discrete adjoint of the step (float32 populations) ----

@@ -1,5 +1,10 @@
 """Post-processing of the solver's output files (the reference's post/ layer).
 
+`profile_metrics` and `profile_objective` restate the mean-profile
+quantities of post/plot_profiles.py (centreline velocity, half-width) for the
+time-averaged radial statistics; the jet adjoint's profile objective uses the
+same definitions (mcg_adjoint_jet_profile_run).
+
 `write_uy_avg_vti` replaces post/binConversionVti.py:12-51, which needs the
 `vtk` package to turn `mean_profiles/uy_avg.bin` (float32, NX*NY*NZ, x
 fastest) into `profiles/uy_avg.vti`.  This one writes the same VTK XML
@@ -72,6 +77,68 @@ def write_uy_avg_vti(case_dir: PathLike, output_dir: Optional[PathLike] = None) 
     output_path.write_text(vti_text(nx, ny, nz, {"uy_avg": data}))
     print(f"uy_avg VTI written to {output_path}")
     return output_path
+
+
+def radial_bin_radii(nx: int, nz: int, nr: int, x0: float, z0: float) -> np.ndarray:
+    """Mean distance from the jet axis of the interior columns of each radial
+    bin, 0 for the first (the numerical centreline), as
+    post/plot_profiles.py:73-91 forms it."""
+    rsum = np.zeros(nr)
+    cnt = np.zeros(nr, np.int64)
+    for x in range(1, nx - 1):
+        for z in range(1, nz - 1):
+            r = float(np.sqrt((float(x) - x0) ** 2 + (float(z) - z0) ** 2))
+            rb = int(r)
+            if rb < nr:
+                rsum[rb] += r
+                cnt[rb] += 1
+    radius = np.arange(nr, dtype=np.float64)
+    np.divide(rsum, cnt, out=radius, where=cnt > 0)
+    radius[0] = 0.0
+    return radius
+
+
+def half_width(profile: np.ndarray, radius: np.ndarray, center_value: float) -> float:
+    """First radius where profile/center_value falls to 1/2, interpolated
+    linearly between bins; NaN when undefined (post/plot_profiles.py:53-70)."""
+    if not np.isfinite(center_value) or center_value <= 0.0:
+        return float("nan")
+    ratio = profile / center_value
+    below = np.where(np.isfinite(ratio) & (ratio <= 0.5))[0]
+    below = below[below > 0]
+    if below.size == 0:
+        return float("nan")
+    i = int(below[0])
+    r1, r2, u1, u2 = radius[i - 1], radius[i], ratio[i - 1], ratio[i]
+    if not np.isfinite(u1) or not np.isfinite(u2) or np.isclose(u1, u2):
+        return float("nan")
+    return float(r1 + (0.5 - u1) * (r2 - r1) / (u2 - u1))
+
+
+def profile_metrics(sum_uy: np.ndarray, count: np.ndarray, nx: int, nz: int, x0: float, z0: float):
+    """Centreline velocity uc[y] (the first annulus) and half-width r_half[y]
+    of the time-averaged radial profiles sum_uy/count ((NY, NR_BINS) or flat)."""
+    nr = nx // 2
+    s = np.asarray(sum_uy, np.float64).reshape(-1, nr)
+    c = np.asarray(count, np.float64).reshape(-1, nr)
+    U = np.full(s.shape, np.nan)
+    np.divide(s, c, out=U, where=c > 0)
+    radius = radial_bin_radii(nx, nz, nr, x0, z0)
+    uc = U[:, 0].copy()
+    rh = np.array([half_width(U[y], radius, uc[y]) for y in range(U.shape[0])])
+    return uc, rh
+
+
+def profile_objective(uc, rh, uc_target, rh_target, y_lo: int, y_hi: int, u_jet: float, diameter: float) -> float:
+    """J = 1/2 sum_{y_lo <= y <= y_hi} ((uc - uc*)/U)^2 + ((r_half - r_half*)/D)^2,
+    each term where both of its values are defined."""
+    J = 0.0
+    for y in range(y_lo, y_hi + 1):
+        if np.isfinite(uc[y]) and np.isfinite(uc_target[y]):
+            J += 0.5 * ((float(uc[y]) - float(uc_target[y])) / u_jet) ** 2
+        if np.isfinite(rh[y]) and np.isfinite(rh_target[y]):
+            J += 0.5 * ((float(rh[y]) - float(rh_target[y])) / diameter) ** 2
+    return J
 
 
 def main() -> None:

@@ -127,6 +127,31 @@ class Solver:
         return {"J": J.value, "dJ_dc": np.array(dc[:], np.float64), "forward_steps": int(fwd.value),
                 "ms": float(ms.value)}
 
+    def adjoint_jet_profile_run(self, nsteps: int, t_begin: int, t_end: int, y_lo: int, y_hi: int, uc_target,
+                                rhalf_target, segment: int = 0) -> Dict:
+        """J = 1/2 sum_{y_lo <= y <= y_hi} ((uc - uc*)/U)^2 + ((r_half - r_half*)/D)^2
+        of the time-averaged centreline velocity and half-width over steps
+        t_begin..t_end, and dJ/dc of the inlet-profile coefficients, from one
+        forward + reverse sweep of the jet; the state is unchanged."""
+        uct = np.ascontiguousarray(uc_target, dtype=np.float32).reshape(-1)
+        rht = np.ascontiguousarray(rhalf_target, dtype=np.float32).reshape(-1)
+        assert uct.size == self.NY and rht.size == self.NY
+        J = C.c_double()
+        dc = (C.c_double * 8)()
+        fwd, ms = C.c_int64(), C.c_float()
+        self._c("mcg_adjoint_jet_profile_run", int(nsteps), int(t_begin), int(t_end), int(y_lo), int(y_hi),
+                _fptr(uct), _fptr(rht), int(segment), C.byref(J), dc, C.byref(fwd), C.byref(ms))
+        return {"J": J.value, "dJ_dc": np.array(dc[:], np.float64), "forward_steps": int(fwd.value),
+                "ms": float(ms.value)}
+
+    def jet_profile_metrics(self):
+        """(uc[NY], r_half[NY]) of the radial statistics accumulated so far:
+        the centreline velocity and the half-width (NaN where undefined)."""
+        uc = np.empty(self.NY, np.float32)
+        rh = np.empty(self.NY, np.float32)
+        self._c("mcg_jet_profile_metrics", _fptr(uc), _fptr(rh))
+        return uc, rh
+
     # -- inlet profile ---------------------------------------------------------
     def set_inlet_bessel(self, coeffs) -> None:
         """Inlet velocity U (1 + sum_k c_k J0(alpha_k r / R)) in jet columns

@@ -15,6 +15,14 @@
 //   ref_dump time <jet|bubble> <warmup> <steps> <stats 0|1>
 //       times <steps> steps with CUDA events on the default stream and prints
 //       one JSON line {"mlups":..,"ms_per_step":..}.
+//   ref_dump outputs <out_dir>
+//       the jet main loop of main.cu:17-120 for the compiled case (NSTEP,
+//       NOUTPUT, NSTATS_START_STEP of the case header), in <out_dir> as the
+//       working directory: the reference's own writers make the JET_VTK tree
+//       (meanF/meanFieldsRT.cuh:93-381, io/save_data.cuh:137-215).
+//   ref_dump vti <fields.bin> <out.vti>
+//       write_vti (io/save_data.cuh:137-200) of the five float32 fields in
+//       <fields.bin> (rhor, rhob, ux, uy, uz, Ncells each); host only.
 
 #include <cstdio>
 #include <cstdlib>
@@ -22,9 +30,13 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 #include "memory.cuh"
 #include "launch.cuh"
 #include "meanF/memoryMeanFields.cuh"
+#include "meanF/meanFieldsRT.cuh"
+#include "io/save_data.cuh"
 #include "utilities/cudaConfig.cuh"
 
 namespace {
@@ -72,6 +84,63 @@ int main(int argc, char **argv) {
         return 2;
     }
     const std::string cmd = argv[1];
+    if (cmd == "vti") {
+        // host only: the reference's VTI writer on given fields
+        if (argc < 4) return 2;
+        const size_t n = size_t(Ncells);
+        std::vector<float> fields(5 * n);
+        if (!read_file(argv[2], fields.data(), fields.size() * 4)) {
+            std::fprintf(stderr, "cannot read %s\n", argv[2]);
+            return 3;
+        }
+        const float *f = fields.data();
+        write_vti(argv[3], f, f + n, f + 2 * n, f + 3 * n, f + 4 * n, true);
+        return 0;
+    }
+    if (cmd == "outputs") {
+        // main.cu:17-120 with the jet initial condition, in <out_dir>
+        if (argc < 3) return 2;
+        if (chdir(argv[2]) != 0) {
+            std::fprintf(stderr, "cannot enter %s\n", argv[2]);
+            return 3;
+        }
+        MeanFieldsRuntime mf{};
+        if (!initialize_mean_fields_runtime(0, mf)) return 4;
+        const CudaConfig cfg = make_cudaConfig();
+        LbmDevice d = allocate_device_memory();
+        LbmHost h = allocate_host_memory();
+        launch_jetDensity(cfg, d);
+        launch_Injet(cfg, d);
+        CUDA_CHECK(cudaDeviceSynchronize());
+        for (int step = 0; step < NSTEP; ++step) {
+            launch_Macros(cfg, d);
+            update_radial_statistics_start(mf, step);
+            if (mf.state.start_uy_average) {
+                launch_accumulate_radial_moments(cfg, d, mf.device);
+                ++mf.state.uy_avg_samples;
+            }
+            launch_collistream(cfg, d);
+            launch_inlet_bc(cfg, d);
+            launch_neumann_bc(cfg, d);
+            if (step % NOUTPUT == 0) {
+                CUDA_CHECK(cudaMemset(mf.device.tke_total, 0, sizeof(real_t)));
+                launch_compute_total_tke(cfg, d, mf.device.tke_total);
+                launch_update_tke_average(mf.device.tke_avg, mf.device.tke_total, step, 0);
+                CUDA_CHECK(cudaDeviceSynchronize());
+                CUDA_CHECK(cudaMemcpy(&mf.host.tke_total, mf.device.tke_total, sizeof(real_t), cudaMemcpyDeviceToHost));
+                CUDA_CHECK(cudaMemcpy(&mf.host.tke_avg, mf.device.tke_avg, sizeof(real_t), cudaMemcpyDeviceToHost));
+                process_tke_sample(mf, step);
+                if (mf.state.start_uy_average && mf.state.uy_avg_samples > 0) write_radial_profile_outputs(mf);
+                if constexpr (write_vti_output) write_vti_step_device(step, d, h);
+            }
+        }
+        CUDA_CHECK(cudaDeviceSynchronize());
+        write_radial_profile_outputs(mf);
+        free_mean_fields_runtime(mf);
+        free_device_memory(d);
+        free_host_memory(h);
+        return 0;
+    }
     CUDA_CHECK(cudaSetDevice(0));
     const CudaConfig cfg = make_cudaConfig();
     LbmDevice d = allocate_device_memory();
