@@ -545,7 +545,8 @@ mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out) {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(out != nullptr, "out is null");
         const mcg::FusedTiling &t = h->tiling;
-        const int32_t v[MCG_TILING_FIELDS] = {t.ty, t.lz, t.tpr, t.ny_tiles, t.nz_chunks, t.smem_bytes, t.pipe, t.fixed_nx};
+        const int32_t v[MCG_TILING_FIELDS] = {t.ty,         t.lz,   t.tpr,      t.ny_tiles, t.nz_chunks,
+                                              t.smem_bytes, t.pipe, t.fixed_nx, t.balanced};
         for (int k = 0; k < MCG_TILING_FIELDS; ++k) out[k] = v[k];
         return MCG_OK;
     });

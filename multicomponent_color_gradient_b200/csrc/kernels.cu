@@ -943,10 +943,6 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     const int lr0 = threadIdx.x / tpr;
     const int lr = lr0 < rpt ? lr0 : T.ty + 2;  // idle groups (tpr not dividing the block) skip every row
     const int x = threadIdx.x - lr0 * tpr;
-    const int y0 = 1 + int(blockIdx.x) * T.ty;
-    const int ty = min(T.ty, g.NY - 1 - y0);
-    const int z0 = 1 + int(blockIdx.y) * T.lz;
-    const int lz = min(T.lz, g.NZ - 1 - z0);
     const int pstride = (T.ty + 2) * tpr;
     const int mplane = T.ty * kMomCount * tpr;
     float *ring = sm;                        // [4][ty+2][tpr]
@@ -954,50 +950,76 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     const C codec = fused_codec<C, kNX>(s_arg, cur);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
-    const bool down = T.alternate && (blockIdx.y & 1);
-    auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
     // Float16 words (27 registers a node) stay in flight across the relaxation
     // of another row: measured +4 % on 128x256x128.  Float32 (27 float2, 54
     // registers) pulls then relaxes: its 3-CTA, 80-register default is faster
     // than the overlap, which spills there.
     constexpr bool kOverlap = std::is_same<C, CodecF16>::value;
-    for (int k = 0; k <= lz + 2; ++k) {
-        const bool do_pull = k <= lz + 1;
-        const int c = k - 2;  // march index of the plane relaxed in this iteration
-        const bool do_relax = c >= 1 && c <= lz;
-        const int zp = plane(k);
-        float *ringp = ring + (k % kPipeRing) * pstride;
-        float *msmp = msm + (k % kPipeStage) * mplane;
-        const bool own_plane = k >= 1 && k <= lz;
-        const int zc = plane(c);
-        const float *pm = ring + (((down ? c + 1 : c - 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc-1
-        const float *p0 = ring + ((c + kPipeRing) % kPipeRing) * pstride;                       // plane zc
-        const float *pp = ring + (((down ? c - 1 : c + 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc+1
-        const float *mc = msm + ((c + kPipeStage) % kPipeStage) * mplane;
-        // rows of this thread: pull rows lr, lr+rpt, ... (< ty+2) and relax rows
-        // 1+lr, 1+lr+rpt, ... (<= ty), interleaved so that a warp has loads of
-        // one row in flight while it relaxes another
-        for (int r = lr; r < ty + 2; r += rpt) {
-            const bool own = own_plane && r >= 1 && r <= ty;
-            const int rc = r + 1;
-            if constexpr (kOverlap) {
-                // the loads of row r are in flight while this warp relaxes row r+1
-                TilePull<C> tp;
-                if (do_pull) tile_pull_issue<C, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, tp);
-                if (do_relax && rc <= ty && xin)
-                    tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
-                if (do_pull)
-                    tile_pull_finish<C, kStats, kPeriodic>(s, codec, x, y0 - 1 + r, zp, own, tp, ringp + r * tpr,
-                                                           msmp + (r - 1) * kMomCount * tpr, tpr);
-            } else {
-                if (do_pull)
-                    tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own, ringp + r * tpr,
-                                                    msmp + (r - 1) * kMomCount * tpr, tpr);
-                if (do_relax && rc <= ty && xin)
-                    tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+    // One march: rows y0 .. y0+ty-1 of planes z0 .. z0+lz-1 (up, or down).
+    auto march = [&](int y0, int z0, int lz, bool down) {
+        const int ty = min(T.ty, g.NY - 1 - y0);
+        auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
+        for (int k = 0; k <= lz + 2; ++k) {
+            const bool do_pull = k <= lz + 1;
+            const int c = k - 2;  // march index of the plane relaxed in this iteration
+            const bool do_relax = c >= 1 && c <= lz;
+            const int zp = plane(k);
+            float *ringp = ring + (k % kPipeRing) * pstride;
+            float *msmp = msm + (k % kPipeStage) * mplane;
+            const bool own_plane = k >= 1 && k <= lz;
+            const int zc = plane(c);
+            const float *pm = ring + (((down ? c + 1 : c - 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc-1
+            const float *p0 = ring + ((c + kPipeRing) % kPipeRing) * pstride;                       // plane zc
+            const float *pp = ring + (((down ? c - 1 : c + 1) + kPipeRing) % kPipeRing) * pstride;  // plane zc+1
+            const float *mc = msm + ((c + kPipeStage) % kPipeStage) * mplane;
+            // rows of this thread: pull rows lr, lr+rpt, ... (< ty+2) and relax rows
+            // 1+lr, 1+lr+rpt, ... (<= ty), interleaved so that a warp has loads of
+            // one row in flight while it relaxes another
+            for (int r = lr; r < ty + 2; r += rpt) {
+                const bool own = own_plane && r >= 1 && r <= ty;
+                const int rc = r + 1;
+                if constexpr (kOverlap) {
+                    // the loads of row r are in flight while this warp relaxes row r+1
+                    TilePull<C> tp;
+                    if (do_pull) tile_pull_issue<C, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, tp);
+                    if (do_relax && rc <= ty && xin)
+                        tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp,
+                                     tpr);
+                    if (do_pull)
+                        tile_pull_finish<C, kStats, kPeriodic>(s, codec, x, y0 - 1 + r, zp, own, tp, ringp + r * tpr,
+                                                               msmp + (r - 1) * kMomCount * tpr, tpr);
+                } else {
+                    if (do_pull)
+                        tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own, ringp + r * tpr,
+                                                        msmp + (r - 1) * kMomCount * tpr, tpr);
+                    if (do_relax && rc <= ty && xin)
+                        tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp,
+                                     tpr);
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
+    };
+    if (T.balanced) {
+        // A resident grid: the tile-planes (y-tile major, then z) are split into
+        // gridDim.x contiguous ranges of equal length, so every CTA does the
+        // same work and no partial wave is left; a range that crosses into the
+        // next y-tile is two marches.  Odd CTAs march down, so neighbouring
+        // ranges reach their shared boundary plane at the same time (L2).
+        const long long nzi = g.NZ - 2;
+        const long long total = (long long)T.ny_tiles * nzi;
+        long long a = (long long)blockIdx.x * total / gridDim.x;
+        const long long b = ((long long)blockIdx.x + 1) * total / gridDim.x;
+        const bool down = T.alternate && (blockIdx.x & 1);
+        while (a < b) {
+            const int tile = int(a / nzi), p0 = int(a % nzi);
+            const int len = int(min(b - a, nzi - p0));
+            march(1 + tile * T.ty, 1 + p0, len, down);
+            a += len;
+        }
+    } else {
+        const int z0 = 1 + int(blockIdx.y) * T.lz;
+        march(1 + int(blockIdx.x) * T.ty, z0, min(T.lz, g.NZ - 1 - z0), T.alternate && (blockIdx.y & 1));
     }
 }
 
@@ -1690,8 +1712,8 @@ cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur,
         return cudaGetLastError();
     }
     if (t.pipe) {
-        k_fused_pipe<C, kStats, kPeriodic, kNX>
-            <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
+        const dim3 grid = t.balanced ? dim3(unsigned(t.balanced)) : dim3(t.ny_tiles, t.nz_chunks);
+        k_fused_pipe<C, kStats, kPeriodic, kNX><<<grid, dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
         return cudaGetLastError();
     }
     k_fused<C, kStats, kPeriodic, kNX>
@@ -2551,6 +2573,27 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     }
     t.alternate = 1;
     if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
+    // the pipelined march on a resident grid of equal contiguous ranges of
+    // tile-planes: CTAs per SM from the register budget and shared memory
+    t.balanced = 0;
+    if (t.pipe == 1) {
+        const int per_sm_regs = g.storage == kStoreF16 ? PipeBlocks<CodecF16>::value : PipeBlocks<CodecF32>::value;
+        const int per_sm_smem = (228 * 1024) / (t.smem_bytes + 1024);
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) {
+            const long long ctas = (long long)sms * std::max(1, std::min(per_sm_regs, per_sm_smem));
+            const long long work = (long long)t.ny_tiles * (g.NZ - 2);
+            // grids of at least four tile-planes per CTA; MCG_FUSED_BALANCED
+            // switches it off (0) or on for any grid (tuning sweeps and the
+            // equality test)
+            const char *v = std::getenv("MCG_FUSED_BALANCED");
+            const bool on = v ? std::atoi(v) != 0 : work >= 4 * ctas;
+            if (on) t.balanced = int(std::min(ctas, work));
+        } else {
+            cudaGetLastError();
+        }
+    }
     // compile-time row length for rows of exactly kFusedNX columns (measured
     // +5 % float32, +10 % float16 on 128x256x128); results are bit-identical
     t.fixed_nx = (g.NX == kFusedNX && t.tpr == kFusedNX) ? kFusedNX : 0;
