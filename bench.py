@@ -390,7 +390,7 @@ def main():
     S, m = measure(args.storage, args.case, args.repeats, args.seconds)
     case, cells, ms, mlups = m["case"], m["cells"], m["ms"], m["mlups"]
     tiling = m["tiling"]
-    kname = {0: "k_fused", 1: "k_fused_pipe", 2: "k_fused_async"}[tiling["pipelined"]]  # the fused-step kernel that ran
+    kname = "k_fused_pipe" if tiling["pipelined"] else "k_fused"  # the fused-step kernel that ran
     codec = "CodecF32" if args.storage == "f32" else "CodecF16"
     traffic, traffic_src = traffic_per_launch(cells, f"{kname}<{codec}>")
     roofline = {"bound": "hbm", "kernel": kname, "achieved": round(m["achieved"], 1), "peak": hbm_peak,

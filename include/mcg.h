@@ -194,7 +194,7 @@ mcg_status mcg_launch_count(const mcg_handle *h, uint64_t *count);
 /* Launch shape of the fused step (no counterpart in the reference, whose
  * launch configuration is fixed): out[0..8] = rows per tile, planes per
  * z chunk, threads per row, y tiles, z chunks, shared memory bytes per CTA,
- * march (1: k_fused_pipe, 2: k_fused_async, 0: k_fused), row length the
+ * march (1: k_fused_pipe, 0: k_fused), row length the
  * kernel is compiled for (0: runtime geometry), CTAs of the resident grid
  * that splits the tile-planes into equal ranges (0: one CTA per tile and
  * z chunk). */

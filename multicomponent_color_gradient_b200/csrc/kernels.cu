@@ -677,27 +677,6 @@ __device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, 
     }
 }
 
-// The global-memory part of tile_store_moments: fluid-plane moments for the
-// boundary launch and the adjoint's moment record.
-template <class C>
-__device__ __forceinline__ void tile_store_moments_global(const DeviceState &s, int x, int y, int zp,
-                                                          const NodeMoments &m, float ps) {
-    const Geometry &g = s.g;
-    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
-        float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
-        const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
-#pragma unroll
-        for (int k = 0; k < kMomCount; ++k) b[size_t(k) * g.NX] = v[k];
-    }
-    if (s.tape) {
-        float *t = s.tape + (uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp));
-        const size_t N = g.N;
-        const float v[kTapePlanes] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, ps};
-#pragma unroll
-        for (int k = 0; k < kTapePlanes; ++k) t[size_t(k) * N] = v[k];
-    }
-}
-
 // One node of a tile row in plane zp, pulled in two halves.  tile_pull_issue
 // loads the node's words (at a position that is not pulled, its psi);
 // tile_pull_finish puts psi into `ring_row` (all columns, halo rows
@@ -955,8 +934,35 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     // registers) pulls then relaxes: its 3-CTA, 80-register default is faster
     // than the overlap, which spills there.
     constexpr bool kOverlap = std::is_same<C, CodecF16>::value;
-    // One march: rows y0 .. y0+ty-1 of planes z0 .. z0+lz-1 (up, or down).
-    auto march = [&](int y0, int z0, int lz, bool down) {
+    // The CTA's marches: rows y0 .. y0+ty-1 of planes z0 .. z0+lz-1 (up, or
+    // down).  One CTA per y-tile and z chunk, or (T.balanced) a resident grid:
+    // the tile-planes (y-tile major, then z) are split into gridDim.x
+    // contiguous ranges of equal length, so every CTA does the same work and
+    // no partial wave is left; a range that crosses into the next y-tile is
+    // two marches.  Odd chunks (odd CTAs of the resident grid) march down, so
+    // neighbouring ranges reach their shared boundary plane at the same time
+    // and the second pull finds it in L2.
+    // (the float16 march, at its 128-register budget, keeps one CTA per tile and chunk)
+    const bool balanced = !kOverlap && T.balanced;
+    const int nzi = g.NZ - 2;
+    const long long total = (long long)T.ny_tiles * nzi;
+    int ra = balanced ? int((long long)blockIdx.x * total / gridDim.x) : 0;
+    const int rb = balanced ? int(((long long)blockIdx.x + 1) * total / gridDim.x) : 1;
+    const bool down = T.alternate && ((balanced ? blockIdx.x : blockIdx.y) & 1);
+    while (ra < rb) {
+        int y0, z0, lz;
+        if (balanced) {
+            const int tile = ra / nzi, p0 = ra - tile * nzi;
+            lz = min(rb - ra, nzi - p0);
+            y0 = 1 + tile * T.ty;
+            z0 = 1 + p0;
+            ra += lz;
+        } else {
+            y0 = 1 + int(blockIdx.x) * T.ty;
+            z0 = 1 + int(blockIdx.y) * T.lz;
+            lz = min(T.lz, g.NZ - 1 - z0);
+            ra = rb;
+        }
         const int ty = min(T.ty, g.NY - 1 - y0);
         auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
         for (int k = 0; k <= lz + 2; ++k) {
@@ -999,215 +1005,6 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
             }
             __syncthreads();
         }
-    };
-    if (T.balanced) {
-        // A resident grid: the tile-planes (y-tile major, then z) are split into
-        // gridDim.x contiguous ranges of equal length, so every CTA does the
-        // same work and no partial wave is left; a range that crosses into the
-        // next y-tile is two marches.  Odd CTAs march down, so neighbouring
-        // ranges reach their shared boundary plane at the same time (L2).
-        const long long nzi = g.NZ - 2;
-        const long long total = (long long)T.ny_tiles * nzi;
-        long long a = (long long)blockIdx.x * total / gridDim.x;
-        const long long b = ((long long)blockIdx.x + 1) * total / gridDim.x;
-        const bool down = T.alternate && (blockIdx.x & 1);
-        while (a < b) {
-            const int tile = int(a / nzi), p0 = int(a % nzi);
-            const int len = int(min(b - a, nzi - p0));
-            march(1 + tile * T.ty, 1 + p0, len, down);
-            a += len;
-        }
-    } else {
-        const int z0 = 1 + int(blockIdx.y) * T.lz;
-        march(1 + int(blockIdx.x) * T.ty, z0, min(T.lz, g.NZ - 1 - z0), T.alternate && (blockIdx.y & 1));
-    }
-}
-
-// ------------------------------------------------------------------ fused step with asynchronous own-row copies
-
-// The march of k_fused_pipe with the moments kept in registers and each
-// node's 27 own-row words fetched one plane ahead by cp.async into shared
-// memory.  A CTA of 256 threads is two row groups of 128 on a 2-row tile
-// (rows of 97 to 128 columns: group 0 pulls halo row 0 and own row 1, group
-// 1 own row 2 and halo row 3), or one group of 256 on a 1-row tile (rows of
-// 129 to 256 columns: halo rows 0 and 2, own row 1); each thread relaxes the
-// node of its own row.  Per plane k:
-//   1. the own row of plane k comes out of this thread's shared-memory stage
-//      (copied during plane k-1): moments, psi, statistics; then the copies
-//      of plane k+1 are issued, so their latency runs under the rest of this
-//      iteration and the next one;
-//   2. the halo rows are pulled directly (colour densities only);
-//   3. one barrier; the node of plane k-1 relaxes from the moments this
-//      thread kept in registers and the psi ring (planes k-2 .. k).
-// A 4-plane psi ring keeps the slot written in step 1 of the next iteration
-// apart from the three the relaxation reads, so one barrier per plane
-// suffices.  The stage is [27][256] words: a warp's copies and reads of one
-// direction are 32 consecutive words.  Results are those of k_fused_pipe bit
-// for bit: the same loads in the same order, decoded and summed the same way.
-constexpr int kAsyncRing = 4;
-
-template <class C>
-struct AsyncBlocks {
-    static constexpr int value = 3;
-};
-
-__device__ __forceinline__ void cp_async_8(void *smem_dst, const void *gsrc) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_4(void *smem_dst, const void *gsrc) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Issue the 27 copies of one node's pull (addresses of `Map`) into the
-// thread's column of the stage.
-template <class C, class Map>
-__device__ __forceinline__ void stage_issue_map(const Map &pm, const C &codec, int x, typename C::Elem *col) {
-    static_for<kQ>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        const typename C::Elem *src = pm.template ptr<i>(codec, x);
-        if constexpr (sizeof(typename C::Elem) == 8)
-            cp_async_8(col + i * kFusedThreads, src);
-        else
-            cp_async_4(col + i * kFusedThreads, src);
-    });
-}
-template <class C, bool kPeriodic>
-__device__ __forceinline__ void stage_issue(const Geometry &g, const C &codec, int x, int y, int z,
-                                            typename C::Elem *col) {
-    if (y >= 2 && y <= g.NY - 3)
-        stage_issue_map(FastPullMap<C>(g, codec, x, y, z), codec, x, col);
-    else
-        stage_issue_map(PullMap<C>(g, x, y, z, kPeriodic), codec, x, col);
-}
-// The staged words as a pull source (moments_from / densities_from).
-template <class C>
-struct StageSource {
-    const C &codec;
-    const typename C::Elem *col;
-    template <int I>
-    __device__ __forceinline__ float2 get(float &gi) const {
-        return codec.template decode<I>(col[I * kFusedThreads], gi);
-    }
-};
-
-// Whether node (x, y, z) of a tile row is pulled, and the coordinates it is
-// pulled at (periodic box: ghosts mirror the wrapped interior node).
-__device__ __forceinline__ bool tile_pulls(const Geometry &g, bool periodic, int x, int y, int z, int &xn, int &yn,
-                                           int &zn) {
-    xn = x;
-    yn = y;
-    zn = z;
-    if (periodic) {
-        xn = wrap_interior(x, g.NX);
-        yn = wrap_interior(y, g.NY);
-        zn = wrap_interior(z, g.NZ);
-        return true;
-    }
-    return x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
-}
-
-template <class C, bool kStats, bool kPeriodic, int kNX, int kG>
-__global__ void __launch_bounds__(kFusedThreads, AsyncBlocks<C>::value) k_fused_async(const DeviceState s_arg,
-                                                                                    const FusedTiling T, int cur,
-                                                                                    int64_t step) {
-    extern __shared__ __align__(16) float sm[];
-    using Elem = typename C::Elem;
-    const DeviceState s = fused_state<C, kNX>(s_arg);
-    const Geometry &g = s.g;
-    const int tpr = kNX > 0 ? kNX : T.tpr;  // kG * tpr == kFusedThreads
-    const int rg = int(threadIdx.x) / tpr;   // row group
-    const int x = int(threadIdx.x) - rg * tpr;
-    const int y0 = 1 + int(blockIdx.x) * kG;
-    const int ty = min(kG, g.NY - 1 - y0);
-    const int z0 = 1 + int(blockIdx.y) * T.lz;
-    const int lz = min(T.lz, g.NZ - 1 - z0);
-    const int pstride = (kG + 2) * tpr;  // one psi plane of the ring: rows 0 .. kG+1
-    float *ring = sm;                    // [4][kG+2][tpr]
-    Elem *col = reinterpret_cast<Elem *>(sm + kAsyncRing * pstride) + threadIdx.x;  // stage column [27][256]
-    const C codec = fused_codec<C, kNX>(s_arg, cur);
-    const float *__restrict__ psi_g = s_arg.psi[step & 1];
-    const bool xin = x >= 1 && x <= g.NX - 2;
-    const bool down = T.alternate && (blockIdx.y & 1);
-    auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
-    // rows of this group: the own row r_own (if within the tile) and the halo
-    // rows: two groups pull rows 0 and 1 / 2 and 3 (a last 1-row tile: group
-    // 1 pulls only halo row 2); one group (256-column rows) pulls rows 0, 1, 2
-    const int r_own = 1 + rg;
-    const bool has_own = r_own <= ty;
-    const int r_halo_a = (kG == 1 || rg == 0) ? 0 : ty + 1;
-    const int y_own = y0 - 1 + r_own;
-    const bool act = x < g.NX;
-
-    // prologue: the own row of march plane 1
-    if (has_own && act && lz >= 1) {
-        int xn, yn, zn;
-        if (tile_pulls(g, kPeriodic, x, y_own, plane(1), xn, yn, zn))
-            stage_issue<C, kPeriodic>(g, codec, xn, yn, zn, col);
-    }
-    cp_async_commit();
-
-    NodeMoments m_prev{};
-    for (int k = 0; k <= lz + 1; ++k) {
-        const int zp = plane(k);
-        const bool own_plane = k >= 1 && k <= lz;
-        float *ringp = ring + (k % kAsyncRing) * pstride;
-        NodeMoments m_new{};
-        // ---- 1. own row (from the stage on own planes, pulled directly on the halo planes)
-        if (has_own) {
-            if (own_plane) {
-                cp_async_wait_all();
-                bool have = false;
-                if (act) {
-                    int xn, yn, zn;
-                    float ps;
-                    if (tile_pulls(g, kPeriodic, x, y_own, zp, xn, yn, zn)) {
-                        m_new = moments_from(StageSource<C>{codec, col});
-                        have = true;
-                        ps = psi_of(m_new.rr, m_new.rb);
-                    } else {
-                        ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y_own) + uint32_t(g.sz) * uint32_t(zp)];
-                    }
-                    ringp[r_own * tpr + x] = ps;
-                    if (xin) tile_store_moments_global<C>(s, x, y_own, zp, m_new, ps);
-                }
-                if constexpr (kStats) radial_accumulate_warp(s, x, y_own, zp, have && xin, m_new.ux, m_new.uy, m_new.uz);
-                // the next plane's copies run under the rest of this plane
-                if (k + 1 <= lz && act) {
-                    int xn, yn, zn;
-                    if (tile_pulls(g, kPeriodic, x, y_own, plane(k + 1), xn, yn, zn))
-                        stage_issue<C, kPeriodic>(g, codec, xn, yn, zn, col);
-                }
-                cp_async_commit();
-            } else {
-                tile_pull<C, false, kPeriodic>(s, codec, psi_g, x, y_own, zp, false, ringp + r_own * tpr, nullptr,
-                                               tpr);
-            }
-        }
-        // ---- 2. halo rows: colour densities only
-        tile_pull<C, false, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r_halo_a, zp, false, ringp + r_halo_a * tpr,
-                                       nullptr, tpr);
-        if constexpr (kG == 1)
-            tile_pull<C, false, kPeriodic>(s, codec, psi_g, x, y0 + 1, zp, false, ringp + 2 * tpr, nullptr, tpr);
-        __syncthreads();
-        // ---- 3. relax the node of plane k-1
-        const int c = k - 1;
-        if (has_own && c >= 1 && c <= lz && xin) {
-            const int zc = plane(c);
-            const float *pm = ring + (((down ? c + 1 : c - 1) + kAsyncRing) % kAsyncRing) * pstride;  // plane zc-1
-            const float *p0 = ring + (c % kAsyncRing) * pstride;                                      // plane zc
-            const float *pp = ring + (((down ? c - 1 : c + 1) + kAsyncRing) % kAsyncRing) * pstride;  // plane zc+1
-            const int base = r_own * tpr + x;
-            auto psi_at = [&](int cx, int cy, int cz) {
-                const float *pl = cz < 0 ? pm : (cz > 0 ? pp : p0);
-                return pl[base + cy * tpr + cx];
-            };
-            collide_node(g, s.ph, codec, pop_row(g, y_own, zc), x, y_own, zc, m_prev, psi_at);
-        }
-        m_prev = m_new;
     }
 }
 
@@ -1684,12 +1481,7 @@ cudaError_t fused_attr_nx(int smem) {
     cudaError_t e = cudaFuncSetAttribute(k_fused<C, kStats, kPeriodic, kNX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_fused_pipe<C, kStats, kPeriodic, kNX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_fused_async<C, kStats, kPeriodic, kNX, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             smem);
-    if (e != cudaSuccess || kNX != 0) return e;
-    return cudaFuncSetAttribute(k_fused_async<C, kStats, kPeriodic, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_fused_pipe<C, kStats, kPeriodic, kNX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem);
 }
 
@@ -1702,15 +1494,6 @@ cudaError_t fused_attr(int smem) {
 
 template <class C, bool kStats, bool kPeriodic, int kNX>
 cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
-    if (t.pipe == 2) {
-        if (kNX == 0 && t.tpr == kFusedThreads)
-            k_fused_async<C, kStats, kPeriodic, 0, 1>
-                <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
-        else
-            k_fused_async<C, kStats, kPeriodic, kNX, 2>
-                <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
-        return cudaGetLastError();
-    }
     if (t.pipe) {
         const dim3 grid = t.balanced ? dim3(unsigned(t.balanced)) : dim3(t.ny_tiles, t.nz_chunks);
         k_fused_pipe<C, kStats, kPeriodic, kNX><<<grid, dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
@@ -2523,9 +2306,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     // with its loads in flight across the relaxation).  Rows of 256 columns
     // need 2-row tiles: the block-synchronous march measured faster there.
     t.pipe = t.tpr <= 128;
-    if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v);  // tuning sweeps: 0, 1, 2
-    // the asynchronous-copy march (pipe 2) takes one or two row groups filling the block
-    if (t.pipe == 2 && t.tpr != kFusedThreads && 2 * t.tpr != kFusedThreads) t.pipe = 1;
+    if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v) != 0;  // tuning sweeps
     if (t.pipe) max_smem = std::max(max_smem, 112 * 1024);  // 4 ring + 3 stage planes: two CTAs per SM
     // rows per tile: at least one round of rows in parallel, 4 by default
     // (measured best on 128x256x128), fewer if shared memory
@@ -2562,21 +2343,12 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     t.nz_chunks = (g.NZ - 2 + lz - 1) / lz;
     t.smem_bytes = t.pipe ? (kPipeRing * (ty + 2) + kPipeStage * kMomCount * ty) * per_row
                           : (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
-    if (t.pipe == 2) {
-        // tiles of one row per group: a 4-plane psi ring of the tile's rows and
-        // their halo rows, and the [27][256] stage of own-row words
-        t.ty = rpt;
-        t.ny_tiles = (g.NY - 2 + t.ty - 1) / t.ty;
-        t.nz_chunks = (g.NZ - 2 + t.lz - 1) / t.lz;
-        const int elem = g.storage == kStoreF16 ? 4 : 8;
-        t.smem_bytes = kAsyncRing * (t.ty + 2) * per_row + kQ * kFusedThreads * elem;
-    }
     t.alternate = 1;
     if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
     // the pipelined march on a resident grid of equal contiguous ranges of
     // tile-planes: CTAs per SM from the register budget and shared memory
     t.balanced = 0;
-    if (t.pipe == 1) {
+    if (t.pipe == 1 && g.storage == kStoreF32) {
         const int per_sm_regs = g.storage == kStoreF16 ? PipeBlocks<CodecF16>::value : PipeBlocks<CodecF32>::value;
         const int per_sm_smem = (228 * 1024) / (t.smem_bytes + 1024);
         int dev = 0, sms = 0;

@@ -208,7 +208,7 @@ def test_periodic_bubble_matches_oracle():
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 @pytest.mark.parametrize("name", ["jet_24x40x24", "bubble_64"])
-@pytest.mark.parametrize("pipe", ["0", "1", "2"])
+@pytest.mark.parametrize("pipe", ["0", "1"])
 def test_fixed_row_length_kernels_equal_runtime_geometry(monkeypatch, storage, name, pipe):
     """Rows of exactly 128 columns run fused kernels compiled for that row
     length (constant slot and row offsets); they produce the populations and
@@ -259,47 +259,14 @@ def test_pipelined_march_equals_block_synchronous_march(monkeypatch, storage, na
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
-@pytest.mark.parametrize("name,shape", [("jet_24x40x24", (128, 24, 38)), ("jet_24x40x24", (100, 21, 36)),
-                                        ("bubble_64", (128, 20, 34)), ("bubble_64", (100, 24, 20)),
-                                        ("jet_24x40x24", (256, 20, 36)), ("bubble_64", (250, 18, 20))])
-def test_async_copy_march_equals_pipelined_march(monkeypatch, storage, name, shape):
-    """k_fused_async (own-row words copied one plane ahead into shared memory
-    by cp.async, moments kept in registers; two row groups on 2-row tiles for
-    rows of up to 128 columns, one group on 1-row tiles for up to 256) does
-    the arithmetic of k_fused_pipe in the same order: equal populations and
-    fields, bit for bit, on 128-, 100-, 256- and 250-column rows (idle
-    lanes), with a 1-row last tile (NY - 2 odd), in both storages, jet and
-    periodic box, 16-plane chunks."""
-    NX, NY, NZ = shape
-    case = get_case(name, NX=NX, NY=NY, NZ=NZ, storage=storage, NSTATS_START_STEP=0)
-    state = initial_state(case, noise=1e-3 if case["boundary"] != "jet" else 0.0, seed=19)
-    monkeypatch.setenv("MCG_FUSED_LZ", "16")
-    out = []
-    for pipe in ("2", "1"):
-        monkeypatch.setenv("MCG_FUSED_PIPE", pipe)
-        with _solver_from_state(case, state) as S:
-            t = S.tiling()
-            assert t["pipelined"] == int(pipe)
-            S.step(25)
-            out.append((S.get_populations(), S.get_fields(), S.get_radial() if case["boundary"] == "jet" else None))
-    (pa, fa, ra), (pb, fb, rb) = out
-    np.testing.assert_array_equal(pa[0], pb[0])
-    np.testing.assert_array_equal(pa[1], pb[1])
-    for k in fa:
-        np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
-    if case["boundary"] == "jet":
-        _radial_close(ra, rb, atol=1e-9)
-
-
-@pytest.mark.parametrize("storage", ["f32", "f16"])
 @pytest.mark.parametrize("name,shape", [("jet_24x40x24", (128, 40, 60)), ("bubble_64", (100, 30, 40)),
                                         ("jet_24x40x24", (256, 20, 36))])
 def test_marches_agree_bit_for_bit(monkeypatch, storage, name, shape):
     """The block-synchronous march, the pipelined march on one CTA per tile
-    and z chunk, and the pipelined march on a resident grid of equal
-    tile-plane ranges (ranges that cross y tiles, 16-plane chunks otherwise)
-    give equal populations and fields, bit for bit, on 128-, 100- and
-    256-column rows, both storages, jet and periodic box."""
+    and z chunk, and (float32) the pipelined march on a resident grid of
+    equal tile-plane ranges (ranges that cross y tiles; 16-plane chunks
+    otherwise) give equal populations and fields, bit for bit, on 128-, 100-
+    and 256-column rows, both storages, jet and periodic box."""
     NX, NY, NZ = shape
     case = get_case(name, NX=NX, NY=NY, NZ=NZ, storage=storage, NSTATS_START_STEP=0)
     state = initial_state(case, noise=1e-3 if case["boundary"] != "jet" else 0.0, seed=29)
@@ -311,7 +278,8 @@ def test_marches_agree_bit_for_bit(monkeypatch, storage, name, shape):
         with _solver_from_state(case, state) as S:
             t = S.tiling()
             assert t["pipelined"] == int(pipe)
-            assert (t["balanced_ctas"] > 0) == (balanced == "1" and pipe == "1")
+            # the resident grid serves the float32 pipelined march
+            assert (t["balanced_ctas"] > 0) == (balanced == "1" and pipe == "1" and storage == "f32")
             S.step(20)
             out.append((S.get_populations(), S.get_fields(), S.get_radial() if case["boundary"] == "jet" else None,
                         t))
