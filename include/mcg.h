@@ -192,13 +192,11 @@ mcg_status mcg_get_step(const mcg_handle *h, int64_t *step);
 /* Kernel launches issued by this handle since creation. */
 mcg_status mcg_launch_count(const mcg_handle *h, uint64_t *count);
 /* Launch shape of the fused step (no counterpart in the reference, whose
- * launch configuration is fixed): out[0..8] = rows per tile, planes per
+ * launch configuration is fixed): out[0..7] = rows per tile, planes per
  * z chunk, threads per row, y tiles, z chunks, shared memory bytes per CTA,
- * march (1: k_fused_pipe, 0: k_fused), row length the
- * kernel is compiled for (0: runtime geometry), CTAs of the resident grid
- * that splits the tile-planes into equal ranges (0: one CTA per tile and
- * z chunk). */
-#define MCG_TILING_FIELDS 9
+ * pipelined march (1: k_fused_pipe, 0: k_fused), row length the kernel is
+ * compiled for (0: runtime geometry). */
+#define MCG_TILING_FIELDS 8
 mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out);
 
 /* ---------------- mean fields and radial statistics (meanF/) ---------------- */

@@ -545,8 +545,7 @@ mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out) {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(out != nullptr, "out is null");
         const mcg::FusedTiling &t = h->tiling;
-        const int32_t v[MCG_TILING_FIELDS] = {t.ty,         t.lz,   t.tpr,      t.ny_tiles, t.nz_chunks,
-                                              t.smem_bytes, t.pipe, t.fixed_nx, t.balanced};
+        const int32_t v[MCG_TILING_FIELDS] = {t.ty, t.lz, t.tpr, t.ny_tiles, t.nz_chunks, t.smem_bytes, t.pipe, t.fixed_nx};
         for (int k = 0; k < MCG_TILING_FIELDS; ++k) out[k] = v[k];
         return MCG_OK;
     });
@@ -637,6 +636,9 @@ mcg_status mcg_get_populations(mcg_handle *h, float *fr, float *fb) {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(fr && fb, "population pointers must not be null");
         if (mcg_status s = mcg::async_flush(h)) return s;
+        // the spare buffer holds the last step's input state, from which the
+        // moment planes the fields report are formed: form them before staging
+        if (mcg_status s = ensure_moments(h)) return s;
         const mcg::Geometry &g = h->s.g;
         const XferPlan x = xfer_plan(h);
         if (x.slots < 1 || x.nchunks > 16) return fail(MCG_ERR_STATE, "transfer plan does not fit the spare buffer");

@@ -934,35 +934,16 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     // registers) pulls then relaxes: its 3-CTA, 80-register default is faster
     // than the overlap, which spills there.
     constexpr bool kOverlap = std::is_same<C, CodecF16>::value;
-    // The CTA's marches: rows y0 .. y0+ty-1 of planes z0 .. z0+lz-1 (up, or
-    // down).  One CTA per y-tile and z chunk, or (T.balanced) a resident grid:
-    // the tile-planes (y-tile major, then z) are split into gridDim.x
-    // contiguous ranges of equal length, so every CTA does the same work and
-    // no partial wave is left; a range that crosses into the next y-tile is
-    // two marches.  Odd chunks (odd CTAs of the resident grid) march down, so
-    // neighbouring ranges reach their shared boundary plane at the same time
-    // and the second pull finds it in L2.
-    // (the float16 march, at its 128-register budget, keeps one CTA per tile and chunk)
-    const bool balanced = !kOverlap && T.balanced;
-    const int nzi = g.NZ - 2;
-    const long long total = (long long)T.ny_tiles * nzi;
-    int ra = balanced ? int((long long)blockIdx.x * total / gridDim.x) : 0;
-    const int rb = balanced ? int(((long long)blockIdx.x + 1) * total / gridDim.x) : 1;
-    const bool down = T.alternate && ((balanced ? blockIdx.x : blockIdx.y) & 1);
-    while (ra < rb) {
-        int y0, z0, lz;
-        if (balanced) {
-            const int tile = ra / nzi, p0 = ra - tile * nzi;
-            lz = min(rb - ra, nzi - p0);
-            y0 = 1 + tile * T.ty;
-            z0 = 1 + p0;
-            ra += lz;
-        } else {
-            y0 = 1 + int(blockIdx.x) * T.ty;
-            z0 = 1 + int(blockIdx.y) * T.lz;
-            lz = min(T.lz, g.NZ - 1 - z0);
-            ra = rb;
-        }
+    // One CTA per y-tile (blockIdx.x) and z chunk (blockIdx.y): CTAs of
+    // neighbouring y-tiles run the same planes at about the same time, so the
+    // halo rows one pulls are the own rows another pulled and hit L2.  Odd
+    // chunks march down: two neighbouring chunks then pull their shared
+    // boundary plane at the same end of their marches (L2 again).
+    {
+        const int y0 = 1 + int(blockIdx.x) * T.ty;
+        const int z0 = 1 + int(blockIdx.y) * T.lz;
+        const int lz = min(T.lz, g.NZ - 1 - z0);
+        const bool down = T.alternate && (blockIdx.y & 1);
         const int ty = min(T.ty, g.NY - 1 - y0);
         auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
         for (int k = 0; k <= lz + 2; ++k) {
@@ -1495,8 +1476,8 @@ cudaError_t fused_attr(int smem) {
 template <class C, bool kStats, bool kPeriodic, int kNX>
 cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
     if (t.pipe) {
-        const dim3 grid = t.balanced ? dim3(unsigned(t.balanced)) : dim3(t.ny_tiles, t.nz_chunks);
-        k_fused_pipe<C, kStats, kPeriodic, kNX><<<grid, dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
+        k_fused_pipe<C, kStats, kPeriodic, kNX>
+            <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
         return cudaGetLastError();
     }
     k_fused<C, kStats, kPeriodic, kNX>
@@ -2345,27 +2326,6 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
                           : (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
     t.alternate = 1;
     if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
-    // the pipelined march on a resident grid of equal contiguous ranges of
-    // tile-planes: CTAs per SM from the register budget and shared memory
-    t.balanced = 0;
-    if (t.pipe == 1 && g.storage == kStoreF32) {
-        const int per_sm_regs = g.storage == kStoreF16 ? PipeBlocks<CodecF16>::value : PipeBlocks<CodecF32>::value;
-        const int per_sm_smem = (228 * 1024) / (t.smem_bytes + 1024);
-        int dev = 0, sms = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess &&
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0) {
-            const long long ctas = (long long)sms * std::max(1, std::min(per_sm_regs, per_sm_smem));
-            const long long work = (long long)t.ny_tiles * (g.NZ - 2);
-            // grids of at least four tile-planes per CTA; MCG_FUSED_BALANCED
-            // switches it off (0) or on for any grid (tuning sweeps and the
-            // equality test)
-            const char *v = std::getenv("MCG_FUSED_BALANCED");
-            const bool on = v ? std::atoi(v) != 0 : work >= 4 * ctas;
-            if (on) t.balanced = int(std::min(ctas, work));
-        } else {
-            cudaGetLastError();
-        }
-    }
     // compile-time row length for rows of exactly kFusedNX columns (measured
     // +5 % float32, +10 % float16 on 128x256x128); results are bit-identical
     t.fixed_nx = (g.NX == kFusedNX && t.tpr == kFusedNX) ? kFusedNX : 0;

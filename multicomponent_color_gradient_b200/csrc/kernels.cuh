@@ -85,7 +85,6 @@ struct FusedTiling {
     int smem_bytes;
     int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
     int pipe;      // software-pipelined march (k_fused_pipe): one barrier per plane
-    int balanced;  // pipelined march on a resident grid of this many CTAs, equal ranges of tile-planes (0: off)
     int fixed_nx;  // row length the kernel is compiled for (0: runtime geometry)
 };
 

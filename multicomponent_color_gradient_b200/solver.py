@@ -321,10 +321,10 @@ class Solver:
 
     def tiling(self) -> dict:
         """Launch shape of the fused step (mcg_get_tiling)."""
-        out = np.zeros(9, np.int32)
+        out = np.zeros(8, np.int32)
         self._c("mcg_get_tiling", out.ctypes.data_as(C.POINTER(C.c_int32)))
         keys = ("rows_per_tile", "planes_per_chunk", "threads_per_row", "y_tiles", "z_chunks", "smem_bytes",
-                "pipelined", "fixed_row_length", "balanced_ctas")
+                "pipelined", "fixed_row_length")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def output_flush(self) -> None:
