@@ -1903,36 +1903,60 @@ __global__ void __launch_bounds__(kBX * kBY, 2) k_adj_collide(const DeviceState 
 template <bool kPeriodic>
 __global__ void __launch_bounds__(kBX * kBY) k_adj_moments(const DeviceState s, const float *__restrict__ M,
                                                           const float *lmom, const float *lf, float *lam_out) {
+    // The block's F-adjoints with a one-node halo, [3][3 planes][kBY+2][kBX+2],
+    // so the 26-neighbour gather reads shared memory.  A halo position holds
+    // lf of the node whose psi it is: periodic neighbours wrap over the
+    // interior; otherwise a position off the interior holds 0 (only interior
+    // nodes relax, and read psi there).
+    constexpr int TX = kBX + 2, TY = kBY + 2, TP = TX * TY * 3;
+    __shared__ float tile[3 * TP];
     const Geometry &g = s.g;
+    const size_t N = g.N;
+    const int bx0 = int(blockIdx.x) * kBX - 1, by0 = int(blockIdx.y) * kBY - 1, bz0 = int(blockIdx.z) - 1;
+    for (int t = threadIdx.y * kBX + threadIdx.x; t < TP; t += kBX * kBY) {
+        const int xt = t % TX, yt = (t / TX) % TY, zt = t / (TX * TY);
+        int xn = bx0 + xt, yn = by0 + yt, zn = bz0 + zt;
+        bool ok;
+        if constexpr (kPeriodic) {
+            ok = xn >= 0 && xn <= g.NX - 1 && yn >= 0 && yn <= g.NY - 1 && zn >= 0 && zn <= g.NZ - 1;
+            xn = wrap_interior(xn, g.NX);
+            yn = wrap_interior(yn, g.NY);
+            zn = wrap_interior(zn, g.NZ);
+        } else {
+            ok = xn >= 1 && xn <= g.NX - 2 && yn >= 1 && yn <= g.NY - 2 && zn >= 1 && zn <= g.NZ - 2;
+        }
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+        if (ok) {
+            const uint32_t nid = uint32_t(xn) + uint32_t(g.sy) * uint32_t(yn) + uint32_t(g.sz) * uint32_t(zn);
+            v0 = lf[0 * N + nid];
+            v1 = lf[1 * N + nid];
+            v2 = lf[2 * N + nid];
+        }
+        tile[t] = v0;
+        tile[TP + t] = v1;
+        tile[2 * TP + t] = v2;
+    }
+    __syncthreads();
     const int x = blockIdx.x * kBX + threadIdx.x;
     const int y = blockIdx.y * kBY + threadIdx.y;
     const int z = blockIdx.z;
     if (!(x >= 1 && x <= g.NX - 2 && y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2)) return;
     const uint32_t id = uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(z);
-    const size_t N = g.N;
     const float *mom = M;
     const float rr = mom[kMomRR * N + id], rb = mom[kMomRB * N + id];
     const float ux = mom[kMomUX * N + id], uy = mom[kMomUY * N + id], uz = mom[kMomUZ * N + id];
     const float rho = rr + rb;
-    // psi(y) enters F(y - c_j) with weight w_j c_j / cs2: periodic neighbours
-    // wrap; otherwise only interior neighbours relax (and read psi(y))
+    // psi(y) enters F(y - c_j) with weight w_j c_j / cs2
     float lpsi = 0.f;
+    const int tc = (1 * TY + int(threadIdx.y) + 1) * TX + int(threadIdx.x) + 1;  // the node in the tile
     static_for<kQ - 1>([&](auto I) {
         constexpr int i = decltype(I)::value + 1;
         using D = Dir<i>;
-        int xn = x - D::cx, yn = y - D::cy, zn = z - D::cz;
-        if constexpr (kPeriodic) {
-            xn = wrap_interior(xn, g.NX);
-            yn = wrap_interior(yn, g.NY);
-            zn = wrap_interior(zn, g.NZ);
-        } else {
-            if (xn < 1 || xn > g.NX - 2 || yn < 1 || yn > g.NY - 2 || zn < 1 || zn > g.NZ - 2) return;
-        }
-        const uint32_t nid = uint32_t(xn) + uint32_t(g.sy) * uint32_t(yn) + uint32_t(g.sz) * uint32_t(zn);
+        const int tn = tc - (D::cz * TY + D::cy) * TX - D::cx;
         float dot = 0.f;
-        if constexpr (D::cx != 0) dot += D::fx * lf[0 * N + nid];
-        if constexpr (D::cy != 0) dot += D::fy * lf[1 * N + nid];
-        if constexpr (D::cz != 0) dot += D::fz * lf[2 * N + nid];
+        if constexpr (D::cx != 0) dot += D::fx * tile[tn];
+        if constexpr (D::cy != 0) dot += D::fy * tile[TP + tn];
+        if constexpr (D::cz != 0) dot += D::fz * tile[2 * TP + tn];
         lpsi += D::w * dot;
     });
     lpsi *= kInvCs2;
