@@ -194,10 +194,20 @@ mcg_status mcg_launch_count(const mcg_handle *h, uint64_t *count);
 /* Launch shape of the fused step (no counterpart in the reference, whose
  * launch configuration is fixed): out[0..7] = rows per tile, planes per
  * z chunk, threads per row, y tiles, z chunks, shared memory bytes per CTA,
- * pipelined march (1: k_fused_pipe, 0: k_fused), row length the kernel is
- * compiled for (0: runtime geometry). */
+ * march (0: k_fused, block-synchronous; 1: k_fused_pipe, pipelined;
+ * 2: k_fused_bulk, pipelined with each pulled row staged in shared memory by
+ * bulk copies; chosen only when the environment sets MCG_FUSED_BULK=1, as it
+ * measured slower), row length the kernel is compiled for (0: runtime
+ * geometry). */
 #define MCG_TILING_FIELDS 8
 mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out);
+/* k_fused_bulk waits for each staged row at most `tries` times (about 1 us
+ * each; default 2^20, about a second).  When a wait runs out, the kernel
+ * finishes its march on stale rows and flags it; the next mcg_synchronize,
+ * mcg_step_timed or mcg_step_profiled returns MCG_ERR_TIMEOUT and the state
+ * must be set again.  tries = 0 makes every wait run out at once (testing
+ * the error path).  No counterpart in the reference. */
+mcg_status mcg_set_stage_wait_limit(mcg_handle *h, int32_t tries);
 
 /* ---------------- mean fields and radial statistics (meanF/) ---------------- */
 

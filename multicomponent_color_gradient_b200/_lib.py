@@ -104,6 +104,7 @@ SIGNATURES = {
     "mcg_output_step_async": [_P, C.c_int32],
     "mcg_output_flush": [_P],
     "mcg_get_tiling": [_P, _I32],
+    "mcg_set_stage_wait_limit": [_P, C.c_int32],
     "mcg_write_radial_outputs": [_P],
     "mcg_write_vti": [_P, C.c_char_p],
     "mcg_write_uy_average": [_P],

@@ -224,6 +224,21 @@ mcg_status one_fused_step(mcg_handle *h, bool *ran_boundary) {
     return MCG_OK;
 }
 
+// After a synchronisation: whether a k_fused_bulk wait for a staged row ran
+// out since the last check (the kernel sets flag[1] and finishes its march on
+// stale rows, so the state is then invalid).  The flag is cleared.
+mcg_status check_stage_waits(mcg_handle *h) {
+    if (!h->tiling.bulk) return MCG_OK;
+    int flag = 0;
+    MCG_CUDA(cudaMemcpyAsync(&flag, h->s.flag + 1, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+             "download wait flag");
+    MCG_CUDA(cudaStreamSynchronize(h->stream), "wait flag");
+    if (!flag) return MCG_OK;
+    MCG_CUDA(cudaMemsetAsync(h->s.flag + 1, 0, sizeof(int), h->stream), "clear wait flag");
+    MCG_CUDA(cudaStreamSynchronize(h->stream), "wait flag");
+    return fail(MCG_ERR_TIMEOUT, "fused step: a wait for a staged row ran out; the state is invalid");
+}
+
 mcg_status run_steps(mcg_handle *h, int32_t nsteps) {
     for (int32_t n = 0; n < nsteps; ++n)
         if (mcg_status s = one_fused_step(h, nullptr)) return s;
@@ -403,6 +418,15 @@ mcg_status mcg_synchronize(mcg_handle *h) {
     return mcg::guarded([&]() -> mcg_status {
         if (mcg_status s = check_handle(h)) return s;
         MCG_CUDA(cudaStreamSynchronize(h->stream), "stream synchronize");
+        return check_stage_waits(h);
+    });
+}
+
+mcg_status mcg_set_stage_wait_limit(mcg_handle *h, int32_t tries) {
+    return mcg::guarded([&]() -> mcg_status {
+        if (mcg_status s = check_handle(h)) return s;
+        MCG_REQUIRE(tries >= 0, "tries must be >= 0");
+        h->tiling.wait_limit = tries;
         return MCG_OK;
     });
 }
@@ -545,7 +569,8 @@ mcg_status mcg_get_tiling(const mcg_handle *h, int32_t *out) {
         if (mcg_status s = check_handle(h)) return s;
         MCG_REQUIRE(out != nullptr, "out is null");
         const mcg::FusedTiling &t = h->tiling;
-        const int32_t v[MCG_TILING_FIELDS] = {t.ty, t.lz, t.tpr, t.ny_tiles, t.nz_chunks, t.smem_bytes, t.pipe, t.fixed_nx};
+        const int32_t march = t.bulk ? 2 : t.pipe;
+        const int32_t v[MCG_TILING_FIELDS] = {t.ty, t.lz, t.tpr, t.ny_tiles, t.nz_chunks, t.smem_bytes, march, t.fixed_nx};
         for (int k = 0; k < MCG_TILING_FIELDS; ++k) out[k] = v[k];
         return MCG_OK;
     });
@@ -785,7 +810,7 @@ mcg_status mcg_step_timed(mcg_handle *h, int32_t nsteps, float *ms) {
         MCG_CUDA(cudaEventRecord(h->ev1, h->stream), "event record");
         MCG_CUDA(cudaEventSynchronize(h->ev1), "event synchronize");
         MCG_CUDA(cudaEventElapsedTime(ms, h->ev0, h->ev1), "event elapsed");
-        return MCG_OK;
+        return check_stage_waits(h);
     });
 }
 
@@ -828,7 +853,7 @@ mcg_status mcg_step_profiled(mcg_handle *h, int32_t nsteps, float *ms_total, flo
             ms_kernels[kind[k]] += ms;
         }
         MCG_CUDA(cudaEventElapsedTime(ms_total, h->prof_events[0], h->prof_events[ev - 1]), "event elapsed");
-        return MCG_OK;
+        return check_stage_waits(h);
     });
 }
 

@@ -637,6 +637,9 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
 // ------------------------------------------------------------------ the fused step
 
 constexpr int kFusedThreads = 256;
+// Row length the fused kernels are specialised for (the 128-column rows of
+// the jet workloads); other row lengths take the runtime-geometry kernels.
+constexpr int kFusedNX = 128;
 
 #ifndef MCG_FUSED_MIN_BLOCKS
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
@@ -1014,6 +1017,300 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
         }
     }
 }
+
+// ------------------------------------------------------------------ bulk-staged pipelined fused step
+
+// One-dimensional bulk copies (cp.async.bulk, no multicast) into shared
+// memory, completed on an mbarrier; one GPU, the CTA's own shared memory.
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Waits for the phase of parity `parity` of `bar` to complete: at most
+// `limit` tries, each suspending the thread for about a microsecond at most.
+// Returns false when the limit ran out (limit 0: at once).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// Barrier of the `count` threads of one row group (named barrier `id` > 0);
+// returns the OR of `pred` over them.
+__device__ __forceinline__ bool group_barrier_or(int id, int count, bool pred) {
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(out)
+        : "r"(uint32_t(pred)), "r"(id), "r"(count)
+        : "memory");
+    return out != 0;
+}
+
+// Row image of a staged pull: the 9 (cy, cz) source segments of row (y, z)
+// (3 slots x NX elements each, group g = dir_group at g*3*NX), copied
+// verbatim from the population buffer.  Direction I of node x reads slot
+// (g, cx+1) at column x - cx, with the lateral wrap of PullMap: columns 1
+// and NX-2 wrap for cx = +1 / -1, except in a segment that comes from a y
+// ghost plane (the boundary's unwrapped slots).
+template <class C, int kNX>
+struct StagedRow {
+    const typename C::Elem *img;
+    int x;
+    int wxp, wxm;
+    bool gy_p, gy_m;
+    __device__ __forceinline__ StagedRow(const typename C::Elem *img_, int x_, int y, const Geometry &g, bool periodic)
+        : img(img_), x(x_) {
+        wxp = (x == 1) ? (kNX - 2) : 0;
+        wxm = (x == kNX - 2) ? -(kNX - 2) : 0;
+        gy_p = !periodic && y == 1;
+        gy_m = !periodic && y == g.NY - 2;
+    }
+    template <int I>
+    __device__ __forceinline__ typename C::Raw load() const {
+        using D = Dir<I>;
+        int xc = 0;
+        if constexpr (D::cx == 1) xc = wxp;
+        if constexpr (D::cx == -1) xc = wxm;
+        if constexpr (D::cy == 1) xc = gy_p ? 0 : xc;
+        if constexpr (D::cy == -1) xc = gy_m ? 0 : xc;
+        return img[(dir_group(I) * C::kGroupSlots + D::cx + 1) * kNX + x - D::cx + xc];
+    }
+};
+
+// Issues the 9 segment copies of pulled row (y, z) (own coordinates, wrapped
+// for the periodic box) into `img`, completing on `bar`.
+template <class C, int kNX>
+__device__ __forceinline__ void stage_row(const Geometry &g, const C &codec, bool periodic, int y, int z,
+                                          typename C::Elem *img, uint64_t *bar) {
+    constexpr uint32_t seg = uint32_t(C::kGroupSlots * kNX * sizeof(typename C::Elem));
+    mbar_expect_tx(bar, 9 * seg);
+    for (int grp = 0; grp < 9; ++grp) {
+        const int cy = grp / 3 - 1, cz = grp % 3 - 1;
+        int ys = y - cy, zs = z - cz;
+        const bool ghost = !periodic && (ys == 0 || ys == g.NY - 1);
+        if (!ghost) {
+            zs = wrap_interior(zs, g.NZ);
+            if (periodic) ys = wrap_interior(ys, g.NY);
+        }
+        const typename C::Elem *src =
+            codec.rd + ((size_t(zs) * g.NY + ys) * kQ + size_t(grp) * C::kGroupSlots) * kNX;
+        bulk_copy_g2s(img + grp * C::kGroupSlots * kNX, src, seg, bar);
+    }
+}
+
+// The pipelined march of k_fused_pipe with each pulled row staged: the 9
+// source segments of a row (3 KB each in float32 at 128 columns) arrive in
+// shared memory by bulk copies while the row group (the 128 threads of one
+// row, 4 warps) finishes its previous row and relaxes another.  Each row
+// group owns one row image and one mbarrier; after its threads have read the
+// image into registers (a barrier of the group), its first thread issues the
+// copies of the group's next pulled row.  Pulls therefore hold no global
+// loads in registers.  Ghost rows and planes are not pulled (psi from HBM).
+// The pulled words, their order and the arithmetic are those of
+// k_fused_pipe, so the results are bit-identical.
+// Every wait has an iteration limit (T.wait_limit tries of about 1 us): when
+// it runs out, the group sets flag[1], issues nothing more and finishes the
+// march on whatever its image holds; before it exits, the group's first
+// thread waits (again bounded) for the copies it has in flight.
+constexpr int kBulkBarBytes = 128;  // mbarriers at the start of the shared memory
+template <class C>
+constexpr int bulk_image_bytes() { return kQ * kFusedNX * int(sizeof(typename C::Elem)); }
+
+template <class C, bool kStats, bool kPeriodic>
+__global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceState s_arg, const FusedTiling T,
+                                                                 int cur, int64_t step) {
+    constexpr int kNX = kFusedNX;
+    constexpr int tpr = kNX;
+    constexpr int rpt = kFusedThreads / tpr;  // row groups
+    using E = typename C::Elem;
+    extern __shared__ __align__(128) unsigned char smb[];
+    const DeviceState s = fused_state<C, kNX>(s_arg);
+    const Geometry &g = s.g;
+    const int grp = threadIdx.x / tpr;
+    const int x = threadIdx.x - grp * tpr;
+    const bool leader = x == 0;
+    const int pstride = (T.ty + 2) * tpr;
+    const int mplane = T.ty * kMomCount * tpr;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smb) + grp;
+    E *img = reinterpret_cast<E *>(smb + kBulkBarBytes) + grp * (kQ * kNX);
+    float *ring = reinterpret_cast<float *>(smb + kBulkBarBytes + rpt * bulk_image_bytes<C>());  // [4][ty+2][tpr]
+    float *msm = ring + kPipeRing * pstride;                                                    // [3][ty][11][tpr]
+    const C codec = fused_codec<C, kNX>(s_arg, cur);
+    const float *__restrict__ psi_g = s_arg.psi[step & 1];
+    const bool xin = x >= 1 && x <= kNX - 2;
+    const int y0 = 1 + int(blockIdx.x) * T.ty;
+    const int z0 = 1 + int(blockIdx.y) * T.lz;
+    const int lz = min(T.lz, g.NZ - 1 - z0);
+    const bool down = T.alternate && (blockIdx.y & 1);
+    const int ty = min(T.ty, g.NY - 1 - y0);
+    auto plane = [&](int k) { return down ? z0 + lz - k : z0 - 1 + k; };
+    // a row of the march that is pulled (the periodic box pulls every row,
+    // ghost rows as their wrapped interior rows)
+    auto pulled = [&](int k, int r) {
+        if constexpr (kPeriodic) return true;
+        const int y = y0 - 1 + r, z = plane(k);
+        return y >= 1 && y <= g.NY - 2 && z >= 1 && z <= g.NZ - 2;
+    };
+    // the group's next pulled row after (k, r); k > lz+1 when there is none
+    auto next_pull = [&](int &k, int &r) {
+        do {
+            r += rpt;
+            if (r >= ty + 2) {
+                r = grp;
+                ++k;
+            }
+        } while (k <= lz + 1 && !pulled(k, r));
+    };
+    auto issue = [&](int k, int r) {
+        int y = y0 - 1 + r, z = plane(k);
+        if constexpr (kPeriodic) {
+            y = wrap_interior(y, g.NY);
+            z = wrap_interior(z, g.NZ);
+        }
+        stage_row<C, kNX>(g, codec, kPeriodic, y, z, img, bar);
+    };
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < rpt; ++k) mbar_init(reinterpret_cast<uint64_t *>(smb) + k, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const uint32_t limit = uint32_t(T.wait_limit);
+    bool failed = false;    // uniform over the row group
+    bool in_flight = false; // leader: copies issued and not yet waited for
+    uint32_t parity = 0;     // of the next phase this thread waits for
+    if (leader && grp < ty + 2) {
+        int k = 0, r = grp;
+        if (!pulled(k, r)) next_pull(k, r);
+        if (k <= lz + 1) {
+            issue(k, r);
+            in_flight = true;
+        }
+    }
+    for (int k = 0; k <= lz + 2; ++k) {
+        const bool do_pull = k <= lz + 1;
+        const int c = k - 2;
+        const bool do_relax = c >= 1 && c <= lz;
+        const int zp = plane(k);
+        float *ringp = ring + (k % kPipeRing) * pstride;
+        float *msmp = msm + (k % kPipeStage) * mplane;
+        const bool own_plane = k >= 1 && k <= lz;
+        const int zc = plane(c);
+        const float *pm = ring + (((down ? c + 1 : c - 1) + kPipeRing) % kPipeRing) * pstride;
+        const float *p0 = ring + ((c + kPipeRing) % kPipeRing) * pstride;
+        const float *pp = ring + (((down ? c - 1 : c + 1) + kPipeRing) % kPipeRing) * pstride;
+        const float *mc = msm + ((c + kPipeStage) % kPipeStage) * mplane;
+        for (int r = grp; r < ty + 2; r += rpt) {
+            const bool own = own_plane && r >= 1 && r <= ty;
+            const int y = y0 - 1 + r;
+            if (do_pull) {
+                if (pulled(k, r)) {
+                    bool late = false;
+                    if (!failed) {
+                        late = !mbar_wait(bar, parity, limit);
+                        if (!late) {
+                            parity ^= 1u;
+                            if (leader) in_flight = false;  // the copies have landed
+                        }
+                    }
+                    int xn = x, yn = y, zn = zp;
+                    if constexpr (kPeriodic) {
+                        xn = wrap_interior(x, kNX);
+                        yn = wrap_interior(y, g.NY);
+                        zn = wrap_interior(zp, g.NZ);
+                    }
+                    const bool pull = kPeriodic || xin;
+                    RawPull<C> raw;
+                    if (pull) {
+                        const StagedRow<C, kNX> src(img, xn, yn, g, kPeriodic);
+                        static_for<kQ>([&](auto I) {
+                            constexpr int i = decltype(I)::value;
+                            raw.v[i] = src.template load<i>();
+                        });
+                    }
+                    // every thread of the group has read the image
+                    const bool now_failed = group_barrier_or(1 + grp, tpr, late);
+                    if (now_failed && !failed) {
+                        failed = true;
+                        if (leader) atomicExch(s.flag + 1, 1);
+                    }
+                    if (leader && !failed) {
+                        int kn = k, rn = r;
+                        next_pull(kn, rn);
+                        if (kn <= lz + 1) {
+                            issue(kn, rn);
+                            in_flight = true;
+                        }
+                    }
+                    NodeMoments m{};
+                    float ps = 0.0f;
+                    if (pull && own) {  // own is uniform per warp
+                        m = moments_from(RawSource<C>{codec, raw});
+                        ps = psi_of(m.rr, m.rb);
+                    } else if (pull) {
+                        float rr, rb;
+                        densities_from(RawSource<C>{codec, raw}, rr, rb);
+                        ps = psi_of(rr, rb);
+                    } else {
+                        ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
+                    }
+                    ringp[r * tpr + x] = ps;
+                    if (own && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msmp + (r - 1) * kMomCount * tpr, tpr);
+                    if constexpr (kStats) {
+                        if (own) radial_accumulate_warp(s, x, y, zp, pull && xin, m.ux, m.uy, m.uz);
+                    }
+                } else {
+                    ringp[r * tpr + x] =
+                        psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
+                }
+            }
+            const int rc = r + 1;
+            if (do_relax && rc <= ty && xin)
+                tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp, tpr);
+        }
+        __syncthreads();
+    }
+    // copies still in flight after a wait ran out land before the CTA exits
+    if (leader && in_flight) mbar_wait(bar, parity, limit > 0 ? limit : kBulkDrainLimit);
+}
+
+// Shared memory of k_fused_bulk with `ty`-row tiles: mbarriers, one row image
+// per row group, the psi ring and the moment stage of k_fused_pipe.
+template <class C>
+constexpr int bulk_smem_for(int ty) {
+    return kBulkBarBytes + (kFusedThreads / kFusedNX) * bulk_image_bytes<C>() +
+           (kPipeRing * (ty + 2) + kPipeStage * kMomCount * ty) * kFusedNX * 4;
+}
+// rows per tile of k_fused_bulk: float32 2 (3 KB segments, 27 KB images),
+// float16 4; both fit two CTAs per SM
+template <class C>
+constexpr int bulk_rows() { return std::is_same<C, CodecF16>::value ? 4 : 2; }
+template <class C>
+constexpr int bulk_smem_bytes() { return bulk_smem_for<C>(bulk_rows<C>()); }
 
 // ------------------------------------------------------------------ granular sequence
 
@@ -1479,9 +1776,6 @@ unsigned grid1(const Geometry &g) {
     return unsigned(want < size_t(8 * 148) ? want : size_t(8 * 148));
 }
 
-// Row length the fused kernels are specialised for (the 128-column rows of
-// the jet workloads); other row lengths take the runtime-geometry kernels.
-constexpr int kFusedNX = 128;
 
 template <class C, bool kStats, bool kPeriodic, int kNX>
 cudaError_t fused_attr_nx(int smem) {
@@ -1496,11 +1790,21 @@ template <class C, bool kStats, bool kPeriodic>
 cudaError_t fused_attr(int smem) {
     cudaError_t e = fused_attr_nx<C, kStats, kPeriodic, 0>(smem);
     if (e != cudaSuccess) return e;
-    return fused_attr_nx<C, kStats, kPeriodic, kFusedNX>(smem);
+    e = fused_attr_nx<C, kStats, kPeriodic, kFusedNX>(smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fused_bulk<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bulk_smem_bytes<C>());
 }
 
 template <class C, bool kStats, bool kPeriodic, int kNX>
 cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
+    if constexpr (kNX == kFusedNX) {
+        if (t.bulk) {
+            k_fused_bulk<C, kStats, kPeriodic>
+                <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
+            return cudaGetLastError();
+        }
+    }
     if (t.pipe) {
         k_fused_pipe<C, kStats, kPeriodic, kNX>
             <<<dim3(t.ny_tiles, t.nz_chunks), dim3(kFusedThreads), size_t(t.smem_bytes), st>>>(s, t, cur, step);
@@ -2363,11 +2667,15 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     int lz = (g.NZ - 2 + chunks - 1) / chunks;
     if (lz < 4) lz = 4;
     if (t.pipe) {
-        // 16-plane chunks (measured best: 1.7 waves of two CTAs per SM on
-        // 128x256x128); grids that give fewer than 1.5 waves at that length keep
-        // the block-synchronous march, whose shorter chunks fill the GPU
+        // Chunks of the pipelined march, measured on 128x256x128 over 8..16
+        // planes: float32 13 planes (10 chunks, 2.9 waves of 3 CTAs per SM;
+        // +4.5 % over 16), float16 10 planes (13 chunks, 2.8 waves of 2 CTAs
+        // per SM; +1 %).  The time follows the fill of the last wave more than
+        // the halo planes.  Grids that give fewer than 1.5 waves of 16-plane
+        // chunks keep the block-synchronous march, whose shorter chunks fill
+        // the GPU.
         const int ctas16 = t.ny_tiles * ((g.NZ - 2 + 15) / 16);
-        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = 16;
+        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = g.storage == kStoreF16 ? 10 : 13;
         else if (!std::getenv("MCG_FUSED_PIPE")) t.pipe = 0;
     }
     if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
@@ -2382,6 +2690,18 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     t.fixed_nx = (g.NX == kFusedNX && t.tpr == kFusedNX) ? kFusedNX : 0;
     if (const char *v = std::getenv("MCG_FUSED_FIXED_NX"))  // tuning sweeps and the equality test
         if (std::atoi(v) == 0) t.fixed_nx = 0;
+    // rows staged by bulk copies (k_fused_bulk), on request only: the
+    // pipelined march on rows of 128 columns (16-byte segments).  Measured on
+    // 128x256x128 it is slower than the register-held pulls (float32 10868
+    // vs 11387 MLUPS, float16 12950 vs 16197): a 27 KB row image per row
+    // group leaves two CTAs per SM with one row in flight each.
+    t.wait_limit = kBulkWaitLimit;
+    const bool f16 = g.storage == kStoreF16;
+    const bool bulk_ok = t.pipe && t.fixed_nx == kFusedNX &&
+                         t.ty <= (f16 ? bulk_rows<CodecF16>() : bulk_rows<CodecF32>());
+    t.bulk = 0;
+    if (const char *v = std::getenv("MCG_FUSED_BULK")) t.bulk = bulk_ok && std::atoi(v) != 0;
+    if (t.bulk) t.smem_bytes = f16 ? bulk_smem_for<CodecF16>(t.ty) : bulk_smem_for<CodecF32>(t.ty);
     return t;
 }
 

@@ -86,7 +86,14 @@ struct FusedTiling {
     int alternate; // odd z-chunks march down, so neighbouring chunks pull their shared planes together
     int pipe;      // software-pipelined march (k_fused_pipe): one barrier per plane
     int fixed_nx;  // row length the kernel is compiled for (0: runtime geometry)
+    int bulk;      // the pipelined march with rows staged by bulk copies (k_fused_bulk)
+    int wait_limit;  // k_fused_bulk: tries (about 1 us each) of a wait for a staged row before it gives up
 };
+
+// Tries of a k_fused_bulk wait by default (about a second), and of the wait
+// for copies still in flight when a CTA gives up.
+constexpr int kBulkWaitLimit = 1 << 20;
+constexpr uint32_t kBulkDrainLimit = 1u << 20;
 
 struct DeviceState {
     Geometry g;
@@ -99,7 +106,7 @@ struct DeviceState {
     float *uy_avg;    // [N]
     double *partials; // reduction scratch
     uint32_t partials_cap;
-    int *flag;        // device flag (non-finite detection)
+    int *flag;        // device flags: [0] non-finite value, [1] a k_fused_bulk wait ran out
     float *tape;      // null, or [kTapePlanes][N]: the fused step records the moments and psi it pulls there
     const float *inlet_profile;  // null (top-hat), or [NZ][NX] multipliers of the inlet velocity per column
 };

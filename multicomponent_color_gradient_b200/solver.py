@@ -327,6 +327,11 @@ class Solver:
                 "pipelined", "fixed_row_length")
         return {k: int(v) for k, v in zip(keys, out)}
 
+    def set_stage_wait_limit(self, tries: int) -> None:
+        """Tries of a staged-row wait of the bulk-staged march
+        (mcg_set_stage_wait_limit; 0 makes every wait run out)."""
+        self._c("mcg_set_stage_wait_limit", int(tries))
+
     def output_flush(self) -> None:
         self._c("mcg_output_flush")
 

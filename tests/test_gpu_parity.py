@@ -286,3 +286,78 @@ def test_marches_agree_bit_for_bit(monkeypatch, storage, name, shape):
             np.testing.assert_array_equal(other[1][k], ref[1][k], err_msg=k)
         if case["boundary"] == "jet":
             _radial_close(other[2], ref[2], atol=1e-9)
+
+
+def _march(monkeypatch, case, state, steps, bulk, lz="16"):
+    """Populations, fields and radial sums after `steps` steps of the pipelined
+    march, with (bulk) or without rows staged by bulk copies."""
+    monkeypatch.setenv("MCG_FUSED_PIPE", "1")
+    monkeypatch.setenv("MCG_FUSED_BULK", "1" if bulk else "0")
+    monkeypatch.setenv("MCG_FUSED_LZ", lz)
+    with _solver_from_state(case, state) as S:
+        t = S.tiling()
+        assert t["pipelined"] == (2 if bulk else 1), t
+        S.step(steps)
+        S.synchronize()
+        return (S.get_populations(), S.get_fields(),
+                S.get_radial() if case["boundary"] == "jet" else None, t)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("name,shape,lz", [("jet_24x40x24", (128, 40, 60), "16"),
+                                           ("jet_24x40x24", (128, 23, 19), "5"),
+                                           ("bubble_64", (128, 30, 40), "16")])
+def test_bulk_staged_march_is_bit_identical(monkeypatch, storage, name, shape, lz):
+    """k_fused_bulk (each pulled row's 9 source segments staged in shared
+    memory by cp.async.bulk) gives the populations, fields and radial sums of
+    k_fused_pipe bit for bit: jet with its ghost rows and planes, a grid whose
+    last tile and chunk are partial, the periodic box with its wrapped rows."""
+    NX, NY, NZ = shape
+    case = get_case(name, NX=NX, NY=NY, NZ=NZ, storage=storage, NSTATS_START_STEP=0)
+    state = initial_state(case, noise=1e-3 if case["boundary"] != "jet" else 0.0, seed=31)
+    ref = _march(monkeypatch, case, state, 20, bulk=False, lz=lz)
+    got = _march(monkeypatch, case, state, 20, bulk=True, lz=lz)
+    np.testing.assert_array_equal(got[0][0], ref[0][0], err_msg=str(got[3]))
+    np.testing.assert_array_equal(got[0][1], ref[0][1], err_msg=str(got[3]))
+    for k in ref[1]:
+        np.testing.assert_array_equal(got[1][k], ref[1][k], err_msg=k)
+    if case["boundary"] == "jet":
+        _radial_close(got[2], ref[2], atol=1e-9)
+
+
+def test_bulk_staged_wait_limit_reports_timeout(monkeypatch):
+    """With a wait limit of 0 tries every wait for a staged row runs out: the
+    kernel flags it, drains its copies in flight and returns, and the next
+    synchronisation reports MCG_ERR_TIMEOUT.  The handle stays usable: with the
+    default limit restored and the state set again, further steps match the
+    pipelined march run through the same sequence of calls."""
+    from multicomponent_color_gradient_b200._lib import McgError
+
+    case = get_case("jet_24x40x24", NX=128, NY=40, NZ=60, NSTATS_START_STEP=0)
+    state = initial_state(case, noise=0.0, seed=37)
+    fr, fb, fields = state
+    monkeypatch.setenv("MCG_FUSED_PIPE", "1")
+    monkeypatch.setenv("MCG_FUSED_LZ", "16")
+    out = {}
+    for bulk in (False, True):
+        monkeypatch.setenv("MCG_FUSED_BULK", "1" if bulk else "0")
+        with _solver_from_state(case, state) as S:
+            assert S.tiling()["pipelined"] == (2 if bulk else 1)
+            if bulk:
+                S.set_stage_wait_limit(0)
+                S.step(3)
+                with pytest.raises(McgError) as err:
+                    S.synchronize()
+                assert err.value.status == 6  # MCG_ERR_TIMEOUT
+                S.synchronize()  # the flag was cleared
+                S.set_stage_wait_limit(1 << 20)
+            else:
+                S.step(3)
+                S.synchronize()
+            S.set_fields(**fields)
+            S.set_populations(fr, fb)
+            S.step(6)
+            S.synchronize()
+            out[bulk] = S.get_populations()
+    np.testing.assert_array_equal(out[True][0], out[False][0])
+    np.testing.assert_array_equal(out[True][1], out[False][1])
