@@ -291,7 +291,8 @@ mcg_status mcg_init_equilibrium(mcg_handle *h, const float *rhor, const float *r
  * returns then).  Reverse sweep with binomial checkpointing in device memory:
  * `snapshots` states are held (S_0 in the handle's own buffer, snapshots-1 more
  * allocated for the call), recomputing forward segments as Griewank's
- * treeverse schedule prescribes.  psi_target: host, Ncells floats (reference
+ * treeverse schedule prescribes, its innermost segments reversed from a tape
+ * of moment records (mcg_set_adjoint_tape, mcg_adjoint_plan_taped).  psi_target: host, Ncells floats (reference
  * node order).  Outputs (any may be NULL): J; dJ/dsigma and dJ/dtau (tau =
  * taur = taub, nu = (tau - 1/2) cs^2); dJ_du0: host, 3*Ncells floats (ux, uy,
  * uz planes, ghost nodes 0) - the gradient with respect to the velocity u0 of
@@ -344,6 +345,16 @@ mcg_status mcg_jet_profile_metrics(mcg_handle *h, float *uc, float *r_half);
  * runs, and the recomputation depth r (least r with C(s + r, s) >= nsteps + 1,
  * s = min(snapshots, nsteps + 1)). */
 mcg_status mcg_adjoint_plan(int32_t nsteps, int32_t snapshots, int64_t *forward_steps, int32_t *sweeps);
+/* The schedule mcg_adjoint_run runs with an adjoint tape of `tape` records
+ * (mcg_set_adjoint_tape): the treeverse splits, with every segment of at
+ * most tape + 1 ops reversed from its held first state by one taped advance
+ * (tape forward steps recording the states' moments, 48 B per node each).
+ * tape = 0 is mcg_adjoint_plan. */
+mcg_status mcg_adjoint_plan_taped(int32_t nsteps, int32_t snapshots, int32_t tape, int64_t *forward_steps,
+                                  int32_t *sweeps);
+/* Records of the taped segments of mcg_adjoint_run (default 20; 0: plain
+ * treeverse, every op forming its record with the moments kernel). */
+mcg_status mcg_set_adjoint_tape(mcg_handle *h, int32_t records);
 
 /* ---------------- output files (io/save_data.cuh, meanF/meanFieldsRT.cuh) ---------------- */
 

@@ -118,6 +118,7 @@ class BubbleProblem:
             raise ValueError("the adjoint covers the periodic box")
         self.nsteps = int(nsteps)
         self.snapshots = int(snapshots) if snapshots else self.nsteps + 1
+        self.tape = None  # records of the taped innermost segments (None: the handle's default)
         self.modes = FourierModes(self.case, max_mode, seed)
         with Solver(self.case) as S:
             S.init_bubble()
@@ -165,7 +166,7 @@ class BubbleProblem:
         S = self.solver(sigma, tau)
         u = self.initial_velocity(a)
         S.init_equilibrium(self.rhor, self.rhob, u[0], u[1], u[2])
-        r = S.adjoint_run(self.target, self.nsteps, self.snapshots)
+        r = S.adjoint_run(self.target, self.nsteps, self.snapshots, self.tape)
         r["dJ_da"] = self.modes.project(r["dJ_du0"])
         return r
 

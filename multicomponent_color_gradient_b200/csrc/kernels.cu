@@ -637,9 +637,11 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
 // ------------------------------------------------------------------ the fused step
 
 constexpr int kFusedThreads = 256;
-// Row length the fused kernels are specialised for (the 128-column rows of
-// the jet workloads); other row lengths take the runtime-geometry kernels.
+// Row lengths the fused kernels are specialised for (the 128-column rows of
+// the 128x256x128 jet, the 256-column rows of the 256x512x256 one); other
+// row lengths take the runtime-geometry kernels.
 constexpr int kFusedNX = 128;
+constexpr int kFusedNX2 = 256;
 
 #ifndef MCG_FUSED_MIN_BLOCKS
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
@@ -1792,6 +1794,8 @@ cudaError_t fused_attr(int smem) {
     if (e != cudaSuccess) return e;
     e = fused_attr_nx<C, kStats, kPeriodic, kFusedNX>(smem);
     if (e != cudaSuccess) return e;
+    e = fused_attr_nx<C, kStats, kPeriodic, kFusedNX2>(smem);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_fused_bulk<C, kStats, kPeriodic>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 bulk_smem_bytes<C>());
 }
@@ -1818,6 +1822,7 @@ cudaError_t fused_launch_nx(const DeviceState &s, const FusedTiling &t, int cur,
 template <class C, bool kStats, bool kPeriodic>
 cudaError_t fused_launch(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, cudaStream_t st) {
     if (t.fixed_nx == kFusedNX) return fused_launch_nx<C, kStats, kPeriodic, kFusedNX>(s, t, cur, step, st);
+    if (t.fixed_nx == kFusedNX2) return fused_launch_nx<C, kStats, kPeriodic, kFusedNX2>(s, t, cur, step, st);
     return fused_launch_nx<C, kStats, kPeriodic, 0>(s, t, cur, step, st);
 }
 
@@ -2685,9 +2690,9 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
                           : (3 * (ty + 2) + 2 * kMomCount * ty) * per_row;
     t.alternate = 1;
     if (const char *v = std::getenv("MCG_FUSED_ALTERNATE")) t.alternate = std::atoi(v) != 0;  // tuning sweeps
-    // compile-time row length for rows of exactly kFusedNX columns (measured
+    // compile-time row length for rows of exactly 128 or 256 columns (measured
     // +5 % float32, +10 % float16 on 128x256x128); results are bit-identical
-    t.fixed_nx = (g.NX == kFusedNX && t.tpr == kFusedNX) ? kFusedNX : 0;
+    t.fixed_nx = ((g.NX == kFusedNX || g.NX == kFusedNX2) && t.tpr == g.NX) ? g.NX : 0;
     if (const char *v = std::getenv("MCG_FUSED_FIXED_NX"))  // tuning sweeps and the equality test
         if (std::atoi(v) == 0) t.fixed_nx = 0;
     // rows staged by bulk copies (k_fused_bulk), on request only: the

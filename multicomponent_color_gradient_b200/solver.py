@@ -166,12 +166,16 @@ class Solver:
         return out.reshape(self.case["NZ"], self.case["NX"])
 
     # -- discrete adjoint (periodic box, float32 storage) ----------------------
-    def adjoint_run(self, psi_target, nsteps: int, snapshots: int) -> Dict:
+    def adjoint_run(self, psi_target, nsteps: int, snapshots: int, tape: Optional[int] = None) -> Dict:
         """J = sum (psi_T - psi_target)^2 over interior nodes after `nsteps`
         steps from the current state, with dJ/dsigma, dJ/dtau and dJ/du0
-        ((3, Ncells) float32) from one reverse sweep; the state is unchanged."""
+        ((3, Ncells) float32) from one reverse sweep; the state is unchanged.
+        `tape`: moment records of the innermost taped segments
+        (mcg_set_adjoint_tape; None keeps the handle's setting, 20 by default)."""
         tgt = np.ascontiguousarray(psi_target, dtype=np.float32).reshape(-1)
         assert tgt.size == self.N
+        if tape is not None:
+            self._c("mcg_set_adjoint_tape", int(tape))
         J, ds, dt = C.c_double(), C.c_double(), C.c_double()
         du0 = np.empty(3 * self.N, np.float32)
         fwd, ms = C.c_int64(), C.c_float()
@@ -353,11 +357,14 @@ class Solver:
         self._c("mcg_output_close")
 
 
-def adjoint_plan(nsteps: int, snapshots: int):
-    """(forward steps, recomputation depth r) of the checkpointing schedule."""
+def adjoint_plan(nsteps: int, snapshots: int, tape: int = 0):
+    """(forward steps, recomputation depth r) of the checkpointing schedule;
+    tape > 0: with taped innermost segments of up to tape + 1 ops (what
+    adjoint_run runs with that tape setting)."""
     lib = _lib.load()
     f, r = C.c_int64(), C.c_int32()
-    _lib.check(lib.mcg_adjoint_plan(int(nsteps), int(snapshots), C.byref(f), C.byref(r)), "mcg_adjoint_plan")
+    _lib.check(lib.mcg_adjoint_plan_taped(int(nsteps), int(snapshots), int(tape), C.byref(f), C.byref(r)),
+               "mcg_adjoint_plan_taped")
     return int(f.value), int(r.value)
 
 

@@ -88,3 +88,45 @@ def test_fourier_modes_eight_per_axis():
     assert abs(lhs - rhs) <= 1e-9 * abs(lhs)
     with pytest.raises(ValueError):
         FourierModes(case, max_mode=11)
+
+
+def taped_forward_steps(n, s, K):
+    """Forward steps of the treeverse splits with every segment of at most
+    K + 1 ops reversed by one taped advance (its length minus one steps)."""
+    from math import comb
+
+    def beta(h, r):
+        return 0 if r < 0 else comb(h + r, h)
+
+    if n <= 1:
+        return 0
+    if n <= K + 1:
+        return n - 1
+    if s == 0:
+        return n * (n - 1) // 2
+    held = s + 1
+    r = 0
+    while beta(held, r) < n:
+        r += 1
+    m = min(max(n - beta(held - 1, r), beta(held, r - 2), 1), n - 1)
+    return m + taped_forward_steps(n - m, s - 1, K) + taped_forward_steps(m, s, K)
+
+
+@pytest.mark.parametrize("tape", [1, 4, 20])
+def test_taped_schedule(tape):
+    """The schedule with taped innermost segments: the count the model above
+    gives, never more than the plain treeverse, T steps once the tape covers
+    the run, and 834 forward steps for the 96^3 bubble's 400 steps with 20
+    held states and 20 records."""
+    for T in list(range(1, 60)) + [100, 400]:
+        for snaps in (1, 2, 3, 5, 20):
+            fwd, _ = adjoint_plan(T, snaps, tape)
+            if snaps > T:
+                assert fwd == T
+                continue
+            assert fwd == taped_forward_steps(T + 1, min(snaps - 1, T), min(tape, T)), (T, snaps, tape)
+            assert fwd <= adjoint_plan(T, snaps)[0]
+            if tape >= T:
+                assert fwd == T
+    if tape == 20:
+        assert adjoint_plan(400, 20, 20)[0] == 834

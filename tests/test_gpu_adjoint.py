@@ -129,15 +129,20 @@ def test_matches_fp64_cpu_adjoint(problem):
 
 
 @pytest.mark.parametrize("snapshots", [2, 5])
-def test_fewer_snapshots_same_gradients(problem, snapshots):
+@pytest.mark.parametrize("tape", [0, 4])
+def test_fewer_snapshots_same_gradients(problem, snapshots, tape):
+    """Binomial checkpointing with 2 or 5 held states, the innermost segments
+    reversed by re-advancing before every op (tape 0) or from a tape of 4
+    moment records: the gradients of the all-states tape, bit for bit for
+    dJ/du0 (the fused step's records equal the moments kernel's)."""
     P, a0 = problem
     full = P.evaluate(a0)
-    P.snapshots = snapshots
+    P.snapshots, P.tape = snapshots, tape
     try:
         r = P.evaluate(a0)
     finally:
-        P.snapshots = T + 1
-    assert r["forward_steps"] == adjoint_plan(T, snapshots)[0] > T
+        P.snapshots, P.tape = T + 1, None
+    assert r["forward_steps"] == adjoint_plan(T, snapshots, tape)[0] > T
     assert abs(r["J"] - full["J"]) <= 1e-12 * full["J"]
     for k in ("dJ_dsigma", "dJ_dtau"):
         assert abs(r[k] - full[k]) <= 1e-9 * abs(full[k])

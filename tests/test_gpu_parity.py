@@ -209,17 +209,19 @@ def test_periodic_bubble_matches_oracle():
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 @pytest.mark.parametrize("name", ["jet_24x40x24", "bubble_64"])
 @pytest.mark.parametrize("pipe", ["0", "1"])
-def test_fixed_row_length_kernels_equal_runtime_geometry(monkeypatch, storage, name, pipe):
-    """Rows of exactly 128 columns run fused kernels compiled for that row
-    length (constant slot and row offsets); they produce the populations and
-    fields of the runtime-geometry kernels bit for bit, in both marches."""
-    case = get_case(name, NX=128, NY=24, NZ=22, storage=storage, NSTATS_START_STEP=0)
+@pytest.mark.parametrize("nx", [128, 256])
+def test_fixed_row_length_kernels_equal_runtime_geometry(monkeypatch, storage, name, pipe, nx):
+    """Rows of exactly 128 or 256 columns run fused kernels compiled for that
+    row length (constant slot and row offsets); they produce the populations
+    and fields of the runtime-geometry kernels bit for bit, in both marches."""
+    case = get_case(name, NX=nx, NY=24, NZ=22, storage=storage, NSTATS_START_STEP=0)
     state = initial_state(case, noise=1e-3 if case["boundary"] != "jet" else 0.0, seed=13)
     monkeypatch.setenv("MCG_FUSED_PIPE", pipe)
     out = []
     for fixed in ("1", "0"):
         monkeypatch.setenv("MCG_FUSED_FIXED_NX", fixed)
         with _solver_from_state(case, state) as S:
+            assert S.tiling()["fixed_row_length"] == (nx if fixed == "1" else 0)
             S.step(30)
             out.append((S.get_populations(), S.get_fields()))
     (pa, fa), (pb, fb) = out
