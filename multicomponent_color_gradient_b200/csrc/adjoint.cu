@@ -174,7 +174,9 @@ struct Run {
     }
 
     // op t with the moment record M of S_t
+    const float *last_record = nullptr;  // the record the latest op read (op 0's, after a sweep)
     mcg_status op_record(const float *M, int64_t t) {
+        last_record = M;
         if (t == T) {
             ADJ_LAUNCH(h, mcg::launch_adj_terminal(base, M, target, lam[lc], acc, h->stream), "adjoint: terminal");
         } else {
@@ -361,8 +363,9 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
         } else {
             if (mcg_status s = run.execute(acts, record_floats)) return s;
         }
-        // op 0 was the last: its record is S_0's
-        const float *M0 = tape_mode ? tape : run.rec;
+        // op 0 was the last: its record is S_0's (the moments kernel's, or a
+        // taped segment's first)
+        const float *M0 = tape_mode ? tape : run.last_record;
         ADJ_LAUNCH(h, mcg::launch_adj_initial(run.base, M0, run.lam[run.lc], du0, h->stream), "adjoint: initial state");
         ADJ_CUDA(cudaEventRecord(h->ev1, h->stream), "event");
         double acc[3] = {0, 0, 0};
@@ -539,7 +542,8 @@ mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t
         }
         ADJ_LAUNCH(h, mcg::launch_fused(d, h->tiling, 0, step0 + t, stats, h->stream), "jet adjoint: forward step");
         d.tape = nullptr;
-        ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
+        if (!h->tiling.boundary)
+            ADJ_LAUNCH(h, mcg::launch_boundary(d, 1, step0 + t, -1, true, h->stream), "jet adjoint: boundary");
         ++fwd;
         return MCG_OK;
     };

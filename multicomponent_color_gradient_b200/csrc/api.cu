@@ -216,7 +216,8 @@ mcg_status one_fused_step(mcg_handle *h, bool *ran_boundary) {
     const bool stats = stats_for_step(h);
     MCG_LAUNCH(h, mcg::launch_fused(h->s, h->tiling, h->cur, h->step, stats, h->stream), "fused step kernel");
     if (stats) ++h->stats_samples;
-    if (jet) MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, true, h->stream), "boundary kernel");
+    if (jet && !h->tiling.boundary)
+        MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, true, h->stream), "boundary kernel");
     if (ran_boundary) *ran_boundary = jet;
     h->cur ^= 1;
     ++h->step;
@@ -836,7 +837,7 @@ mcg_status mcg_step_profiled(mcg_handle *h, int32_t nsteps, float *ms_total, flo
             if (stats) ++h->stats_samples;
             MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
             kind.push_back(0);
-            if (jet) {
+            if (jet && !h->tiling.boundary) {
                 MCG_LAUNCH(h, mcg::launch_boundary(h->s, h->cur ^ 1, h->step, -1, true, h->stream), "boundary kernel");
                 MCG_CUDA(cudaEventRecord(h->prof_events[ev++], h->stream), "event record");
                 kind.push_back(1);

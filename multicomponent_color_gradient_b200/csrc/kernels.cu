@@ -1,6 +1,7 @@
 // kernels.cu - the D3Q27 colour-gradient step on B200 (sm_100a).
 //
-// The step is one HBM pass (k_fused) plus a plane-sized launch (k_boundary):
+// The step is one HBM pass, one launch (k_fused, or its pipelined forms
+// k_fused_pipe and k_fused_bulk):
 //   k_fused    a CTA owns a tile of rows (y) and marches a chunk of z planes.
 //              For each plane it pulls f(t) for its rows plus a one-row halo
 //              from the population buffer (row-blocked layout, so a pulled row
@@ -13,11 +14,13 @@
 //              same step's psi in shared memory (the reference needs a kernel
 //              boundary for this), storing the post-collision values at each
 //              node (pull layout, coalesced rows).  Moments never go to HBM.
-//   k_boundary the inlet (jet/boundary_conditions.cuh:17-85) and convective
-//              outlet (jet/boundary_conditions.cuh:163-233) of the same step,
-//              one thread per boundary column, from the fluid-plane moments
-//              k_fused leaves in bmom; values land in the y ghost planes of
+//              The threads of the fluid rows 1 and NY-2 also write the jet's
+//              inlet (jet/boundary_conditions.cuh:17-85) and convective outlet
+//              (:163-233) columns of the same step into the y ghost planes of
 //              the new buffer.
+//   k_boundary the same boundary as a launch of its own, one thread per
+//              column, from the fluid-plane moments the step leaves in bmom
+//              (the granular sequence, and MCG_FUSED_BOUNDARY=0).
 // The granular launch sequence of the reference (k_moments, k_collide,
 // k_boundary, k_accumulate_radial) is kept for callers that drive the
 // launchers one by one; it writes the moment planes to HBM like the reference.
@@ -99,8 +102,10 @@ struct CodecF32 {
 // 2 min(fr,fb)/g carrying the sign of fr-fb.  Pure nodes store q = +-0
 // exactly, so a single-colour region keeps exactly zero of the other colour.
 __device__ __forceinline__ __half2 f16_encode(float r, float b, float inv_w, float rho0) {
-    const float g = r + b;
-    const float h0 = g * inv_w - rho0;
+    // rounded operation by operation, so that every kernel that inlines it
+    // (the jet boundary is written from several) gives the same word
+    const float g = __fadd_rn(r, b);
+    const float h0 = __fsub_rn(__fmul_rn(g, inv_w), rho0);
     const float mn = fminf(r, b);
     float q = (g > 0.0f) ? __fdividef(2.0f * mn, g) : 0.0f;
     q = copysignf(fmaxf(q, 0.0f), r - b);
@@ -201,7 +206,7 @@ __device__ __forceinline__ float omega_at(const Physics &ph, int y) {
 
 __device__ __forceinline__ bool is_jet_column(const Physics &ph, int x, int z) {  // mathUtilities.cuh:14-21
     const float dx = float(x) - ph.jet_x0, dz = float(z) - ph.jet_z0;
-    return dx * dx + dz * dz <= ph.jet_r2;
+    return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)) <= ph.jet_r2;
 }
 
 // Inlet velocity of jet column (x, z): the top-hat U (boundary_conditions.cuh:62),
@@ -213,7 +218,7 @@ __device__ __forceinline__ float inlet_velocity(const DeviceState &s, int64_t st
     if (s.inlet_profile) U *= s.inlet_profile[x + s.g.NX * z];
     if (ph.inlet_noise == 0.0f) return U;
     const float u = hash_uniform(ph.seed, 0x1A1E7ull ^ uint64_t(step), uint64_t(x), uint64_t(z));
-    return U * (1.0f + (2.0f * u - 1.0f) * ph.inlet_noise);
+    return __fmul_rn(U, __fadd_rn(1.0f, __fmul_rn(__fsub_rn(2.0f * u, 1.0f), ph.inlet_noise)));
 }
 
 __host__ __device__ __forceinline__ int wrap_interior(int v, int n) { return v == 0 ? n - 2 : (v == n - 1 ? 1 : v); }
@@ -634,6 +639,145 @@ __device__ __forceinline__ void radial_accumulate_warp(const DeviceState &s, int
     }
 }
 
+// ------------------------------------------------------------------ boundary arithmetic
+
+// The jet boundary columns are written from every fused kernel (and from
+// k_boundary).  Their arithmetic is rounded operation by operation (no
+// contraction into fused multiply-adds, which the compiler chooses per
+// kernel), so that every kernel writes the same bits.  Same formulas as
+// make_eq, make_neq, feq and fneq (lbm.cuh:16-78).
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+
+__device__ __forceinline__ EqTerms bnd_eq(float ux, float uy, float uz) {
+    return EqTerms{ux, uy, uz, radd(radd(rmul(ux, ux), rmul(uy, uy)), rmul(uz, uz))};
+}
+__device__ __forceinline__ NeqTerms bnd_neq(const NodeMoments &m) {
+    NeqTerms n;
+    n.pxx = m.pxx; n.pxy = m.pxy; n.pyy = m.pyy; n.pyz = m.pyz; n.pzz = m.pzz; n.pxz = m.pxz;
+    n.a3xxy = radd(rmul(m.pxx, m.uy), rmul(2.0f * m.pxy, m.ux));
+    n.a3xxz = radd(rmul(m.pxx, m.uz), rmul(2.0f * m.pxz, m.ux));
+    n.a3xyy = radd(rmul(m.pyy, m.ux), rmul(2.0f * m.pxy, m.uy));
+    n.a3xzz = radd(rmul(m.pzz, m.ux), rmul(2.0f * m.pxz, m.uz));
+    n.a3yyz = radd(rmul(m.pyy, m.uz), rmul(2.0f * m.pyz, m.uy));
+    n.a3yzz = radd(rmul(m.pzz, m.uy), rmul(2.0f * m.pyz, m.uz));
+    n.a3xyz = radd(radd(rmul(m.pxy, m.uz), rmul(m.pxz, m.uy)), rmul(m.pyz, m.ux));
+    return n;
+}
+template <int I>
+__device__ __forceinline__ float bnd_feq(float rho, const EqTerms &e) {
+    using D = Dir<I>;
+    float cu = 0.0f;
+    if constexpr (D::cx != 0) cu = radd(cu, D::fx * e.ux);
+    if constexpr (D::cy != 0) cu = radd(cu, D::fy * e.uy);
+    if constexpr (D::cz != 0) cu = radd(cu, D::fz * e.uz);
+    const float cu2 = rmul(cu, cu);
+    const float A2 = radd(rsub(rmul(cu2, kInv2Cs4), rmul(e.usq, kInv2Cs2)), rmul(cu, kInvCs2));
+    const float A3 = rmul(cu, rsub(rmul(cu2, kInv6Cs6), rmul(e.usq, kInv2Cs4)));
+    return rmul(rmul(D::w, rho), radd(radd(1.0f, A2), A3));
+}
+template <int I>
+__device__ __forceinline__ float bnd_fneq(const NeqTerms &n) {
+    using D = Dir<I>;
+    float A2 = 0.0f;
+    if constexpr (D::Hxx != 0.0f) A2 = radd(A2, rmul(n.pxx, D::Hxx));
+    if constexpr (D::Hxy != 0.0f) A2 = radd(A2, rmul(2.0f * n.pxy, D::Hxy));
+    if constexpr (D::Hyy != 0.0f) A2 = radd(A2, rmul(n.pyy, D::Hyy));
+    if constexpr (D::Hyz != 0.0f) A2 = radd(A2, rmul(2.0f * n.pyz, D::Hyz));
+    if constexpr (D::Hzz != 0.0f) A2 = radd(A2, rmul(n.pzz, D::Hzz));
+    if constexpr (D::Hxz != 0.0f) A2 = radd(A2, rmul(2.0f * n.pxz, D::Hxz));
+    A2 = rmul(A2, kInv2Cs4);
+    float A3 = 0.0f;
+    if constexpr (D::Hxxy != 0.0f) A3 = radd(A3, rmul(n.a3xxy, D::Hxxy));
+    if constexpr (D::Hxxz != 0.0f) A3 = radd(A3, rmul(n.a3xxz, D::Hxxz));
+    if constexpr (D::Hxyy != 0.0f) A3 = radd(A3, rmul(n.a3xyy, D::Hxyy));
+    if constexpr (D::Hxzz != 0.0f) A3 = radd(A3, rmul(n.a3xzz, D::Hxzz));
+    if constexpr (D::Hyyz != 0.0f) A3 = radd(A3, rmul(n.a3yyz, D::Hyyz));
+    if constexpr (D::Hyzz != 0.0f) A3 = radd(A3, rmul(n.a3yzz, D::Hyzz));
+    if constexpr (D::Hxyz != 0.0f) A3 = radd(A3, rmul(2.0f * n.a3xyz, D::Hxyz));
+    return rmul(D::w, radd(A2, rmul(A3, kInv2Cs6)));
+}
+// omega_at with the same rounding rule (the outlet's fluid plane)
+__device__ __forceinline__ float bnd_omega_at(const Physics &ph, int y) {
+    if (!ph.sponge) return ph.omega;
+    const float s = clamp01(rmul(float(y) - ph.sponge_y_start, ph.sponge_inv_width));
+    const float nus = rmul(ph.nu, radd(1.0f, rmul(ph.sponge_K, rmul(rmul(s, s), s))));
+    return 1.0f / radd(0.5f, rmul(nus, kInvCs2));
+}
+
+// ------------------------------------------------------------------ boundary pieces
+
+// Inlet column (x,z): density mask at y=0 and, for disc columns, the nine
+// cy=+1 populations entering y=1 (jet/boundary_conditions.cuh:17-85).  They
+// are stored in the ghost plane y=0 of `dst` at (x,0,z), where the y=1 nodes
+// (x+cx, 1, z+cz) pull them.  `m` are the moments of fluid node (x,1,z).
+template <class C>
+__device__ __forceinline__ void inlet_column(const DeviceState &s, void *dst, float *psi_dst, int x, int z,
+                                             int64_t step, const NodeMoments &m) {
+    const Geometry &g = s.g;
+    const Physics &ph = s.ph;
+    const uint32_t idB = uint32_t(x) + uint32_t(g.sz) * uint32_t(z);
+    const bool jet = is_jet_column(ph, x, z);
+    const float rrB = (1.0f - (jet ? 1.0f : 0.0f)) * ph.rhor0;
+    const float rbB = (jet ? 1.0f : 0.0f) * ph.rhob0;
+    s.mom[size_t(kMomRR) * g.N + idB] = rrB;
+    s.mom[size_t(kMomRB) * g.N + idB] = rbB;
+    psi_dst[idB] = psi_of(rrB, rbB);
+    if (!jet) return;
+    const float rT = radd(rrB, rbB);
+    const float aR = rmul(rrB, 1.0f / rT), aB = rmul(rbB, 1.0f / rT);
+    const float oms = rsub(1.0f, ph.omega_b);
+    const EqTerms e = bnd_eq(0.0f, inlet_velocity(s, step, x, z), 0.0f);
+    const NeqTerms n = bnd_neq(m);
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (Dir<i>::cy == 1) {
+            const float gi = radd(bnd_feq<i>(rT, e), rmul(oms, bnd_fneq<i>(n)));
+            C::store_to(dst, g, i, x, 0, z, rmul(aR, gi), rmul(aB, gi), ph.f16_rho0);
+        }
+    });
+}
+
+// Outlet column (x,z): convective update of the y=NY-1 state from fluid node
+// F=(x,NY-2,z) and the nine cy=-1 populations entering y=NY-2
+// (jet/boundary_conditions.cuh:163-233), stored in ghost plane y=NY-1 of dst.
+template <class C>
+__device__ __forceinline__ void outlet_column(const DeviceState &s, void *dst, float *psi_dst, int x, int z,
+                                              const NodeMoments &m) {
+    const Geometry &g = s.g;
+    const Physics &ph = s.ph;
+    const uint32_t idB = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 1) + uint32_t(g.sz) * uint32_t(z);
+    float *mom = s.mom;
+    const size_t N = g.N;
+    const float uc = clamp01(m.uy);
+    auto conv = [uc](float b, float f) { return rsub(b, rmul(uc, rsub(b, f))); };
+    const float rrB = conv(mom[kMomRR * N + idB], m.rr);
+    const float rbB = conv(mom[kMomRB * N + idB], m.rb);
+    const float uxB = conv(mom[kMomUX * N + idB], m.ux);
+    const float uyB = conv(mom[kMomUY * N + idB], m.uy);
+    const float uzB = conv(mom[kMomUZ * N + idB], m.uz);
+    mom[kMomRR * N + idB] = rrB;
+    mom[kMomRB * N + idB] = rbB;
+    mom[kMomUX * N + idB] = uxB;
+    mom[kMomUY * N + idB] = uyB;
+    mom[kMomUZ * N + idB] = uzB;
+    psi_dst[idB] = psi_of(rrB, rbB);
+    const float rhoT = radd(rrB, rbB);
+    const float inv = 1.0f / rhoT;
+    const float aR = rmul(rrB, inv), aB = rmul(rbB, inv);
+    const float oms = rsub(1.0f, bnd_omega_at(ph, g.NY - 2));
+    const EqTerms e = bnd_eq(uxB, uyB, uzB);
+    const NeqTerms n = bnd_neq(m);
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr (Dir<i>::cy == -1) {
+            const float gi = radd(bnd_feq<i>(rhoT, e), rmul(oms, bnd_fneq<i>(n)));
+            C::store_to(dst, g, i, x, g.NY - 1, z, rmul(aR, gi), rmul(aB, gi), ph.f16_rho0);
+        }
+    });
+}
+
 // ------------------------------------------------------------------ the fused step
 
 constexpr int kFusedThreads = 256;
@@ -649,9 +793,45 @@ constexpr int kFusedNX2 = 256;
 
 // Own-row results of a pulled node: the moments into the stage row, the
 // fluid-plane moments for the boundary launch, the adjoint's moment record.
+// First row of this CTA's y-tile.  With the jet boundary in the step the
+// tiles are numbered from the outlet end: the outlet tile's CTAs, which also
+// write the outlet columns, then start first in each chunk instead of last.
+// Neighbouring CTAs still hold neighbouring tiles.
+__device__ __forceinline__ int tile_y0(const FusedTiling &T) {
+    const int t = T.boundary ? T.ny_tiles - 1 - int(blockIdx.x) : int(blockIdx.x);
+    return 1 + t * T.ty;
+}
+
+// Where the fused step puts the jet boundary of its step: dst == nullptr, the
+// fluid-plane moments into bmom for k_boundary; otherwise the boundary
+// columns themselves (inlet_column / outlet_column into the ghost planes of
+// dst, the buffer the step writes, and into psi_next), from the own-row
+// thread of each fluid node of rows 1 and NY-2.  A column reads and writes
+// only its own ghost nodes and the outlet state it carries, none of which the
+// same step reads, so it needs no ordering against the rest of the launch.
+struct BoundaryOut {
+    void *dst;
+    float *psi_next;
+    int64_t step;
+};
+__device__ __forceinline__ BoundaryOut boundary_out(const DeviceState &s_arg, const FusedTiling &T, int cur,
+                                                    int64_t step) {
+    if (!T.boundary) return BoundaryOut{nullptr, nullptr, step};
+    return BoundaryOut{s_arg.pops[cur ^ 1], s_arg.psi[(step + 1) & 1], step};
+}
+
+// The boundary columns of a fused step (kept inline: out of line, the call
+// puts the kernel's state on the stack).
+template <class C>
+__device__ __forceinline__ void fused_boundary_column(const DeviceState &s, const BoundaryOut &bo, int x, int y, int zp,
+                                                   const NodeMoments &m) {
+    if (y == 1) inlet_column<C>(s, bo.dst, bo.psi_next, x, zp, bo.step, m);
+    if (y == s.g.NY - 2) outlet_column<C>(s, bo.dst, bo.psi_next, x, zp, m);
+}
+
 template <class C>
 __device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, int y, int zp, const NodeMoments &m,
-                                                   float ps, float *msm_row, int tpr) {
+                                                   float ps, float *msm_row, int tpr, const BoundaryOut &bo) {
     const Geometry &g = s.g;
     float *q = msm_row + x;
     q[kMomRR * tpr] = m.rr;
@@ -665,7 +845,9 @@ __device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, 
     q[kMomPYZ * tpr] = m.pyz;
     q[kMomPZZ * tpr] = m.pzz;
     q[kMomPXZ * tpr] = m.pxz;
-    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
+    if (g.boundary == kBoundaryJet && bo.dst && (y == 1 || y == g.NY - 2)) {
+        fused_boundary_column<C>(s, bo, x, y, zp, m);
+    } else if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
         // fluid-plane moments for the boundary launch
         float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
         const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
@@ -728,7 +910,7 @@ struct RadialSample {
 template <class C, bool kStats, bool kPeriodic>
 __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &codec, int x, int y, int zp,
                                                  bool own_row, const TilePull<C> &t, float *ring_row, float *msm_row,
-                                                 int tpr, RadialSample *defer = nullptr) {
+                                                 int tpr, const BoundaryOut &bo, RadialSample *defer = nullptr) {
     const Geometry &g = s.g;
     const bool xin = x >= 1 && x <= g.NX - 2;
     NodeMoments m{};
@@ -747,7 +929,7 @@ __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &
             ps = t.ps;
         }
         ring_row[x] = ps;
-        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr, bo);
     }
     if constexpr (kStats) {
         if (defer) {
@@ -764,7 +946,8 @@ __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &
 // branch keeps every word live at once and spills at 80 registers).
 template <class C, bool kStats, bool kPeriodic>
 __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, const float *__restrict__ psi_g, int x,
-                                          int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr) {
+                                          int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr,
+                                          const BoundaryOut &bo) {
     const Geometry &g = s.g;
     const bool xin = x >= 1 && x <= g.NX - 2;
     NodeMoments m{};
@@ -793,7 +976,7 @@ __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, 
             ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
         }
         ring_row[x] = ps;
-        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr, bo);
     }
     if constexpr (kStats) {
         if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
@@ -864,7 +1047,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     const int lr0 = threadIdx.x / tpr;
     const int lr = lr0 < rpt ? lr0 : T.ty + 2;
     const int x = threadIdx.x - lr0 * tpr;
-    const int y0 = 1 + int(blockIdx.x) * T.ty;
+    const int y0 = tile_y0(T);
     const int ty = min(T.ty, g.NY - 1 - y0);
     const int z0 = 1 + int(blockIdx.y) * T.lz;
     const int lz = min(T.lz, g.NZ - 1 - z0);
@@ -873,6 +1056,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     float *msm = sm + 3 * pstride;         // [2][ty][11][tpr]
     const int mplane = T.ty * kMomCount * tpr;
     const C codec = fused_codec<C, kNX>(s_arg, cur);
+    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
     // Odd chunks march down: the plane two neighbouring chunks both pull (one
@@ -887,7 +1071,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
         for (int r = lr; r < ty + 2; r += rpt) {
             tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
-                                            ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
+                                            ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr, bo);
         }
         __syncthreads();
         // ---- relax the plane behind the march front, whose neighbours are all pulled
@@ -943,6 +1127,7 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     float *ring = sm;                        // [4][ty+2][tpr]
     float *msm = sm + kPipeRing * pstride;   // [3][ty][11][tpr]
     const C codec = fused_codec<C, kNX>(s_arg, cur);
+    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
     // Float16 words (27 registers a node) stay in flight across the relaxation
@@ -956,7 +1141,7 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     // chunks march down: two neighbouring chunks then pull their shared
     // boundary plane at the same end of their marches (L2 again).
     {
-        const int y0 = 1 + int(blockIdx.x) * T.ty;
+        const int y0 = tile_y0(T);
         const int z0 = 1 + int(blockIdx.y) * T.lz;
         const int lz = min(T.lz, g.NZ - 1 - z0);
         const bool down = T.alternate && (blockIdx.y & 1);
@@ -999,14 +1184,14 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
                                      tpr);
                     if (do_pull) {
                         tile_pull_finish<C, kStats, kPeriodic>(s, codec, x, y0 - 1 + r, zp, own, tp, ringp + r * tpr,
-                                                               msmp + (r - 1) * kMomCount * tpr, tpr,
+                                                               msmp + (r - 1) * kMomCount * tpr, tpr, bo,
                                                                kStats && own ? &held : nullptr);
                         if (kStats && own) pending = true;
                     }
                 } else {
                     if (do_pull)
                         tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own, ringp + r * tpr,
-                                                        msmp + (r - 1) * kMomCount * tpr, tpr);
+                                                        msmp + (r - 1) * kMomCount * tpr, tpr, bo);
                     if (do_relax && rc <= ty && xin)
                         tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp,
                                      tpr);
@@ -1163,9 +1348,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceSta
     float *ring = reinterpret_cast<float *>(smb + kBulkBarBytes + rpt * bulk_image_bytes<C>());  // [4][ty+2][tpr]
     float *msm = ring + kPipeRing * pstride;                                                    // [3][ty][11][tpr]
     const C codec = fused_codec<C, kNX>(s_arg, cur);
+    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];
     const bool xin = x >= 1 && x <= kNX - 2;
-    const int y0 = 1 + int(blockIdx.x) * T.ty;
+    const int y0 = tile_y0(T);
     const int z0 = 1 + int(blockIdx.y) * T.lz;
     const int lz = min(T.lz, g.NZ - 1 - z0);
     const bool down = T.alternate && (blockIdx.y & 1);
@@ -1281,7 +1467,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceSta
                         ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
                     }
                     ringp[r * tpr + x] = ps;
-                    if (own && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msmp + (r - 1) * kMomCount * tpr, tpr);
+                    if (own && xin)
+                        tile_store_moments<C>(s, x, y, zp, m, ps, msmp + (r - 1) * kMomCount * tpr, tpr, bo);
                     if constexpr (kStats) {
                         if (own) radial_accumulate_warp(s, x, y, zp, pull && xin, m.ux, m.uy, m.uz);
                     }
@@ -1384,78 +1571,6 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_collide(const DeviceState s, c
     const float *__restrict__ psi = s.psi[step & 1];
     auto psi_at = [&](int cx, int cy, int cz) { return __ldg(psi + (int(id) + cx + g.sy * cy + g.sz * cz)); };
     collide_node(g, s.ph, codec, pop_row(g, y, z), x, y, z, m, psi_at);
-}
-
-// ------------------------------------------------------------------ boundary pieces
-
-// Inlet column (x,z): density mask at y=0 and, for disc columns, the nine
-// cy=+1 populations entering y=1 (jet/boundary_conditions.cuh:17-85).  They
-// are stored in the ghost plane y=0 of `dst` at (x,0,z), where the y=1 nodes
-// (x+cx, 1, z+cz) pull them.  `m` are the moments of fluid node (x,1,z).
-template <class C>
-__device__ __forceinline__ void inlet_column(const DeviceState &s, void *dst, float *psi_dst, int x, int z,
-                                             int64_t step, const NodeMoments &m) {
-    const Geometry &g = s.g;
-    const Physics &ph = s.ph;
-    const uint32_t idB = uint32_t(x) + uint32_t(g.sz) * uint32_t(z);
-    const bool jet = is_jet_column(ph, x, z);
-    const float rrB = (1.0f - (jet ? 1.0f : 0.0f)) * ph.rhor0;
-    const float rbB = (jet ? 1.0f : 0.0f) * ph.rhob0;
-    s.mom[size_t(kMomRR) * g.N + idB] = rrB;
-    s.mom[size_t(kMomRB) * g.N + idB] = rbB;
-    psi_dst[idB] = psi_of(rrB, rbB);
-    if (!jet) return;
-    const float rT = rrB + rbB;
-    const float aR = rrB * (1.0f / rT), aB = rbB * (1.0f / rT);
-    const float oms = 1.0f - ph.omega_b;
-    const EqTerms e = make_eq(0.0f, inlet_velocity(s, step, x, z), 0.0f);
-    const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
-    static_for<kQ>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        if constexpr (Dir<i>::cy == 1) {
-            const float gi = feq<i>(rT, e) + oms * fneq<i>(n);
-            C::store_to(dst, g, i, x, 0, z, aR * gi, aB * gi, ph.f16_rho0);
-        }
-    });
-}
-
-// Outlet column (x,z): convective update of the y=NY-1 state from fluid node
-// F=(x,NY-2,z) and the nine cy=-1 populations entering y=NY-2
-// (jet/boundary_conditions.cuh:163-233), stored in ghost plane y=NY-1 of dst.
-template <class C>
-__device__ __forceinline__ void outlet_column(const DeviceState &s, void *dst, float *psi_dst, int x, int z,
-                                              const NodeMoments &m) {
-    const Geometry &g = s.g;
-    const Physics &ph = s.ph;
-    const uint32_t idB = uint32_t(x) + uint32_t(g.sy) * uint32_t(g.NY - 1) + uint32_t(g.sz) * uint32_t(z);
-    float *mom = s.mom;
-    const size_t N = g.N;
-    const float uc = clamp01(m.uy);
-    auto conv = [uc](float b, float f) { return b - uc * (b - f); };
-    const float rrB = conv(mom[kMomRR * N + idB], m.rr);
-    const float rbB = conv(mom[kMomRB * N + idB], m.rb);
-    const float uxB = conv(mom[kMomUX * N + idB], m.ux);
-    const float uyB = conv(mom[kMomUY * N + idB], m.uy);
-    const float uzB = conv(mom[kMomUZ * N + idB], m.uz);
-    mom[kMomRR * N + idB] = rrB;
-    mom[kMomRB * N + idB] = rbB;
-    mom[kMomUX * N + idB] = uxB;
-    mom[kMomUY * N + idB] = uyB;
-    mom[kMomUZ * N + idB] = uzB;
-    psi_dst[idB] = psi_of(rrB, rbB);
-    const float rhoT = rrB + rbB;
-    const float inv = 1.0f / rhoT;
-    const float aR = rrB * inv, aB = rbB * inv;
-    const float oms = 1.0f - omega_at(ph, g.NY - 2);
-    const EqTerms e = make_eq(uxB, uyB, uzB);
-    const NeqTerms n = make_neq(m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz, m.ux, m.uy, m.uz);
-    static_for<kQ>([&](auto I) {
-        constexpr int i = decltype(I)::value;
-        if constexpr (Dir<i>::cy == -1) {
-            const float gi = feq<i>(rhoT, e) + oms * fneq<i>(n);
-            C::store_to(dst, g, i, x, g.NY - 1, z, aR * gi, aB * gi, ph.f16_rho0);
-        }
-    });
 }
 
 __device__ __forceinline__ NodeMoments load_moments(const float *m, size_t stride, size_t id) {
@@ -2701,6 +2816,10 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     // vs 11387 MLUPS, float16 12950 vs 16197): a 27 KB row image per row
     // group leaves two CTAs per SM with one row in flight each.
     t.wait_limit = kBulkWaitLimit;
+    // the jet's inlet and outlet columns from the fused step's own-row threads
+    // of rows 1 and NY-2, instead of a k_boundary launch after it
+    t.boundary = g.boundary == kBoundaryJet;
+    if (const char *v = std::getenv("MCG_FUSED_BOUNDARY")) t.boundary = t.boundary && std::atoi(v) != 0;  // tests
     const bool f16 = g.storage == kStoreF16;
     const bool bulk_ok = t.pipe && t.fixed_nx == kFusedNX &&
                          t.ty <= (f16 ? bulk_rows<CodecF16>() : bulk_rows<CodecF32>());

@@ -88,6 +88,7 @@ struct FusedTiling {
     int fixed_nx;  // row length the kernel is compiled for (0: runtime geometry)
     int bulk;      // the pipelined march with rows staged by bulk copies (k_fused_bulk)
     int wait_limit;  // k_fused_bulk: tries (about 1 us each) of a wait for a staged row before it gives up
+    int boundary;    // jet: the fused step writes the inlet and outlet columns itself (no k_boundary launch)
 };
 
 // Tries of a k_fused_bulk wait by default (about a second), and of the wait

@@ -363,3 +363,38 @@ def test_bulk_staged_wait_limit_reports_timeout(monkeypatch):
             out[bulk] = S.get_populations()
     np.testing.assert_array_equal(out[True][0], out[False][0])
     np.testing.assert_array_equal(out[True][1], out[False][1])
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("march", ["0", "1", "bulk"])
+@pytest.mark.parametrize("shape", [(128, 40, 60), (100, 30, 40)])
+def test_boundary_in_the_fused_step_equals_the_boundary_launch(monkeypatch, storage, march, shape):
+    """The jet's inlet and outlet columns written by the fused step's own-row
+    threads of rows 1 and NY-2 equal those of a separate k_boundary launch
+    after the step, bit for bit: populations, fields (the outlet's carried
+    state and the inlet mask included) and radial sums, with the seeded inlet
+    perturbation, in every march and both storages."""
+    NX, NY, NZ = shape
+    if march == "bulk" and NX != 128:
+        pytest.skip("the bulk-staged march runs 128-column rows")
+    case = get_case("jet_24x40x24", NX=NX, NY=NY, NZ=NZ, storage=storage, NSTATS_START_STEP=0,
+                    inlet_noise=0.01, seed=5)
+    state = initial_state(case, noise=0.0, seed=41)
+    monkeypatch.setenv("MCG_FUSED_PIPE", "0" if march == "0" else "1")
+    monkeypatch.setenv("MCG_FUSED_BULK", "1" if march == "bulk" else "0")
+    monkeypatch.setenv("MCG_FUSED_LZ", "8")
+    out = []
+    for fused in ("1", "0"):
+        monkeypatch.setenv("MCG_FUSED_BOUNDARY", fused)
+        with _solver_from_state(case, state) as S:
+            l0 = S.launches
+            S.step(12)
+            launches = S.launches - l0
+            out.append((S.get_populations(), S.get_fields(), S.get_radial(), launches))
+    (pa, fa, ra, la), (pb, fb, rb, lb) = out
+    assert (la, lb) == (12, 24)
+    np.testing.assert_array_equal(pa[0], pb[0])
+    np.testing.assert_array_equal(pa[1], pb[1])
+    for k in fa:
+        np.testing.assert_array_equal(fa[k], fb[k], err_msg=k)
+    _radial_close(ra, rb, atol=1e-9)
