@@ -14,10 +14,10 @@
 //              same step's psi in shared memory (the reference needs a kernel
 //              boundary for this), storing the post-collision values at each
 //              node (pull layout, coalesced rows).  Moments never go to HBM.
-//              The threads of the fluid rows 1 and NY-2 also write the jet's
-//              inlet (jet/boundary_conditions.cuh:17-85) and convective outlet
-//              (:163-233) columns of the same step into the y ghost planes of
-//              the new buffer.
+//              The CTAs whose tiles hold the fluid rows 1 and NY-2 then write
+//              the jet's inlet (jet/boundary_conditions.cuh:17-85) and
+//              convective outlet (:163-233) columns of their chunk into the y
+//              ghost planes of the new buffer (fused_boundary).
 //   k_boundary the same boundary as a launch of its own, one thread per
 //              column, from the fluid-plane moments the step leaves in bmom
 //              (the granular sequence, and MCG_FUSED_BOUNDARY=0).
@@ -706,6 +706,15 @@ __device__ __forceinline__ float bnd_omega_at(const Physics &ph, int y) {
     return 1.0f / radd(0.5f, rmul(nus, kInvCs2));
 }
 
+__device__ __forceinline__ NodeMoments load_moments(const float *m, size_t stride, size_t id) {
+    NodeMoments r;
+    r.rr = m[kMomRR * stride + id]; r.rb = m[kMomRB * stride + id];
+    r.ux = m[kMomUX * stride + id]; r.uy = m[kMomUY * stride + id]; r.uz = m[kMomUZ * stride + id];
+    r.pxx = m[kMomPXX * stride + id]; r.pxy = m[kMomPXY * stride + id]; r.pyy = m[kMomPYY * stride + id];
+    r.pyz = m[kMomPYZ * stride + id]; r.pzz = m[kMomPZZ * stride + id]; r.pxz = m[kMomPXZ * stride + id];
+    return r;
+}
+
 // ------------------------------------------------------------------ boundary pieces
 
 // Inlet column (x,z): density mask at y=0 and, for disc columns, the nine
@@ -791,8 +800,6 @@ constexpr int kFusedNX2 = 256;
 #define MCG_FUSED_MIN_BLOCKS 3  // CTAs per SM the register budget is sized for
 #endif
 
-// Own-row results of a pulled node: the moments into the stage row, the
-// fluid-plane moments for the boundary launch, the adjoint's moment record.
 // First row of this CTA's y-tile.  With the jet boundary in the step the
 // tiles are numbered from the outlet end: the outlet tile's CTAs, which also
 // write the outlet columns, then start first in each chunk instead of last.
@@ -802,36 +809,12 @@ __device__ __forceinline__ int tile_y0(const FusedTiling &T) {
     return 1 + t * T.ty;
 }
 
-// Where the fused step puts the jet boundary of its step: dst == nullptr, the
-// fluid-plane moments into bmom for k_boundary; otherwise the boundary
-// columns themselves (inlet_column / outlet_column into the ghost planes of
-// dst, the buffer the step writes, and into psi_next), from the own-row
-// thread of each fluid node of rows 1 and NY-2.  A column reads and writes
-// only its own ghost nodes and the outlet state it carries, none of which the
-// same step reads, so it needs no ordering against the rest of the launch.
-struct BoundaryOut {
-    void *dst;
-    float *psi_next;
-    int64_t step;
-};
-__device__ __forceinline__ BoundaryOut boundary_out(const DeviceState &s_arg, const FusedTiling &T, int cur,
-                                                    int64_t step) {
-    if (!T.boundary) return BoundaryOut{nullptr, nullptr, step};
-    return BoundaryOut{s_arg.pops[cur ^ 1], s_arg.psi[(step + 1) & 1], step};
-}
-
-// The boundary columns of a fused step (kept inline: out of line, the call
-// puts the kernel's state on the stack).
-template <class C>
-__device__ __forceinline__ void fused_boundary_column(const DeviceState &s, const BoundaryOut &bo, int x, int y, int zp,
-                                                   const NodeMoments &m) {
-    if (y == 1) inlet_column<C>(s, bo.dst, bo.psi_next, x, zp, bo.step, m);
-    if (y == s.g.NY - 2) outlet_column<C>(s, bo.dst, bo.psi_next, x, zp, m);
-}
-
+// Own-row results of a pulled node: the moments into the stage row, the
+// fluid-plane moments for the boundary (fused_boundary or k_boundary), the
+// adjoint's moment record.
 template <class C>
 __device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, int y, int zp, const NodeMoments &m,
-                                                   float ps, float *msm_row, int tpr, const BoundaryOut &bo) {
+                                                   float ps, float *msm_row, int tpr) {
     const Geometry &g = s.g;
     float *q = msm_row + x;
     q[kMomRR * tpr] = m.rr;
@@ -845,9 +828,7 @@ __device__ __forceinline__ void tile_store_moments(const DeviceState &s, int x, 
     q[kMomPYZ * tpr] = m.pyz;
     q[kMomPZZ * tpr] = m.pzz;
     q[kMomPXZ * tpr] = m.pxz;
-    if (g.boundary == kBoundaryJet && bo.dst && (y == 1 || y == g.NY - 2)) {
-        fused_boundary_column<C>(s, bo, x, y, zp, m);
-    } else if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
+    if (g.boundary == kBoundaryJet && (y == 1 || y == g.NY - 2)) {
         // fluid-plane moments for the boundary launch
         float *b = s.bmom + ((size_t(y == 1 ? 0 : 1) * g.NZ + zp) * kMomCount) * g.NX + x;
         const float v[kMomCount] = {m.rr, m.rb, m.ux, m.uy, m.uz, m.pxx, m.pxy, m.pyy, m.pyz, m.pzz, m.pxz};
@@ -910,7 +891,7 @@ struct RadialSample {
 template <class C, bool kStats, bool kPeriodic>
 __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &codec, int x, int y, int zp,
                                                  bool own_row, const TilePull<C> &t, float *ring_row, float *msm_row,
-                                                 int tpr, const BoundaryOut &bo, RadialSample *defer = nullptr) {
+                                                 int tpr, RadialSample *defer = nullptr) {
     const Geometry &g = s.g;
     const bool xin = x >= 1 && x <= g.NX - 2;
     NodeMoments m{};
@@ -929,7 +910,7 @@ __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &
             ps = t.ps;
         }
         ring_row[x] = ps;
-        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr, bo);
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
     }
     if constexpr (kStats) {
         if (defer) {
@@ -946,8 +927,7 @@ __device__ __forceinline__ void tile_pull_finish(const DeviceState &s, const C &
 // branch keeps every word live at once and spills at 80 registers).
 template <class C, bool kStats, bool kPeriodic>
 __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, const float *__restrict__ psi_g, int x,
-                                          int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr,
-                                          const BoundaryOut &bo) {
+                                          int y, int zp, bool own_row, float *ring_row, float *msm_row, int tpr) {
     const Geometry &g = s.g;
     const bool xin = x >= 1 && x <= g.NX - 2;
     NodeMoments m{};
@@ -976,7 +956,7 @@ __device__ __forceinline__ void tile_pull(const DeviceState &s, const C &codec, 
             ps = psi_g[uint32_t(x) + uint32_t(g.sy) * uint32_t(y) + uint32_t(g.sz) * uint32_t(zp)];
         }
         ring_row[x] = ps;
-        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr, bo);
+        if (own_row && xin) tile_store_moments<C>(s, x, y, zp, m, ps, msm_row, tpr);
     }
     if constexpr (kStats) {
         if (own_row) radial_accumulate_warp(s, x, y, zp, have && xin, m.ux, m.uy, m.uz);
@@ -1010,6 +990,36 @@ __device__ __forceinline__ void tile_collide(const DeviceState &s, const C &code
         return pl[base + cy * tpr + cx];
     };
     collide_node(g, s.ph, codec, pop_row(g, y, zc), x, y, zc, m, psi_at);
+}
+
+// The jet boundary of a fused step, from the CTAs whose tile holds fluid row
+// 1 (inlet) or NY-2 (outlet), once their march is over: every column of the
+// chunk from the fluid-plane moments the march left in bmom (written by this
+// CTA's threads, visible after the barrier), into the ghost planes of the
+// buffer the step writes and the next step's psi.  A column touches only its
+// own ghost nodes and the outlet state it carries, which no other CTA of the
+// launch reads.  Kept out of the march, where it added its instructions to
+// every row.  The condition is uniform over the CTA.
+template <class C>
+__device__ __forceinline__ void fused_boundary(const DeviceState &s, const FusedTiling &T, int y0, int ty, int z0,
+                                               int lz) {
+    const Geometry &g = s.g;
+    const bool inlet = y0 == 1, outlet = y0 + ty - 1 == g.NY - 2;
+    if (!T.boundary || !(inlet || outlet)) return;
+    __syncthreads();
+    const int nx = g.NX - 2;
+    for (int side = 0; side < 2; ++side) {
+        if (!(side == 0 ? inlet : outlet)) continue;
+        for (int i = threadIdx.x; i < lz * nx; i += blockDim.x) {
+            const int x = 1 + i % nx, z = z0 + i / nx;
+            const NodeMoments m =
+                load_moments(s.bmom + (size_t(side) * g.NZ + z) * kMomCount * g.NX, size_t(g.NX), size_t(x));
+            if (side == 0)
+                inlet_column<C>(s, T.bnd_dst, T.bnd_psi, x, z, int64_t(T.bnd_step), m);
+            else
+                outlet_column<C>(s, T.bnd_dst, T.bnd_psi, x, z, m);
+        }
+    }
 }
 
 // Geometry of a fused launch: with kNX > 0 (rows of exactly kNX columns, one
@@ -1056,7 +1066,6 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
     float *msm = sm + 3 * pstride;         // [2][ty][11][tpr]
     const int mplane = T.ty * kMomCount * tpr;
     const C codec = fused_codec<C, kNX>(s_arg, cur);
-    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
     // Odd chunks march down: the plane two neighbouring chunks both pull (one
@@ -1071,7 +1080,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         // ---- pull plane zp: psi for rows y0-1 .. y0+ty, moments for own rows
         for (int r = lr; r < ty + 2; r += rpt) {
             tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own_plane && r >= 1 && r <= ty,
-                                            ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr, bo);
+                                            ringp + r * tpr, msmp + (r - 1) * kMomCount * tpr, tpr);
         }
         __syncthreads();
         // ---- relax the plane behind the march front, whose neighbours are all pulled
@@ -1088,6 +1097,7 @@ __global__ void __launch_bounds__(kFusedThreads, MCG_FUSED_MIN_BLOCKS) k_fused(c
         }
         __syncthreads();
     }
+    fused_boundary<C>(s, T, y0, ty, z0, lz);
 }
 
 // ------------------------------------------------------------------ software-pipelined fused step
@@ -1127,7 +1137,6 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
     float *ring = sm;                        // [4][ty+2][tpr]
     float *msm = sm + kPipeRing * pstride;   // [3][ty][11][tpr]
     const C codec = fused_codec<C, kNX>(s_arg, cur);
-    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];  // indexed on the parameter, not the local copy
     const bool xin = x >= 1 && x <= g.NX - 2;
     // Float16 words (27 registers a node) stay in flight across the relaxation
@@ -1184,14 +1193,14 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
                                      tpr);
                     if (do_pull) {
                         tile_pull_finish<C, kStats, kPeriodic>(s, codec, x, y0 - 1 + r, zp, own, tp, ringp + r * tpr,
-                                                               msmp + (r - 1) * kMomCount * tpr, tpr, bo,
+                                                               msmp + (r - 1) * kMomCount * tpr, tpr,
                                                                kStats && own ? &held : nullptr);
                         if (kStats && own) pending = true;
                     }
                 } else {
                     if (do_pull)
                         tile_pull<C, kStats, kPeriodic>(s, codec, psi_g, x, y0 - 1 + r, zp, own, ringp + r * tpr,
-                                                        msmp + (r - 1) * kMomCount * tpr, tpr, bo);
+                                                        msmp + (r - 1) * kMomCount * tpr, tpr);
                     if (do_relax && rc <= ty && xin)
                         tile_collide(s, codec, x, y0 - 1 + rc, zc, rc, mc + (rc - 1) * kMomCount * tpr, pm, p0, pp,
                                      tpr);
@@ -1202,6 +1211,7 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
         if constexpr (kStats) {
             if (pending) radial_accumulate_warp(s, x, held.y, held.z, held.active, held.ux, held.uy, held.uz);
         }
+        fused_boundary<C>(s, T, y0, ty, z0, lz);
     }
 }
 
@@ -1348,7 +1358,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceSta
     float *ring = reinterpret_cast<float *>(smb + kBulkBarBytes + rpt * bulk_image_bytes<C>());  // [4][ty+2][tpr]
     float *msm = ring + kPipeRing * pstride;                                                    // [3][ty][11][tpr]
     const C codec = fused_codec<C, kNX>(s_arg, cur);
-    const BoundaryOut bo = boundary_out(s_arg, T, cur, step);
     const float *__restrict__ psi_g = s_arg.psi[step & 1];
     const bool xin = x >= 1 && x <= kNX - 2;
     const int y0 = tile_y0(T);
@@ -1468,7 +1477,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceSta
                     }
                     ringp[r * tpr + x] = ps;
                     if (own && xin)
-                        tile_store_moments<C>(s, x, y, zp, m, ps, msmp + (r - 1) * kMomCount * tpr, tpr, bo);
+                        tile_store_moments<C>(s, x, y, zp, m, ps, msmp + (r - 1) * kMomCount * tpr, tpr);
                     if constexpr (kStats) {
                         if (own) radial_accumulate_warp(s, x, y, zp, pull && xin, m.ux, m.uy, m.uz);
                     }
@@ -1485,6 +1494,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2) k_fused_bulk(const DeviceSta
     }
     // copies still in flight after a wait ran out land before the CTA exits
     if (leader && in_flight) mbar_wait(bar, parity, limit > 0 ? limit : kBulkDrainLimit);
+    fused_boundary<C>(s, T, y0, ty, z0, lz);
 }
 
 // Shared memory of k_fused_bulk with `ty`-row tiles: mbarriers, one row image
@@ -1573,14 +1583,6 @@ __global__ void __launch_bounds__(kBX * kBY, 4) k_collide(const DeviceState s, c
     collide_node(g, s.ph, codec, pop_row(g, y, z), x, y, z, m, psi_at);
 }
 
-__device__ __forceinline__ NodeMoments load_moments(const float *m, size_t stride, size_t id) {
-    NodeMoments r;
-    r.rr = m[kMomRR * stride + id]; r.rb = m[kMomRB * stride + id];
-    r.ux = m[kMomUX * stride + id]; r.uy = m[kMomUY * stride + id]; r.uz = m[kMomUZ * stride + id];
-    r.pxx = m[kMomPXX * stride + id]; r.pxy = m[kMomPXY * stride + id]; r.pyy = m[kMomPYY * stride + id];
-    r.pyz = m[kMomPYZ * stride + id]; r.pzz = m[kMomPZZ * stride + id]; r.pxz = m[kMomPXZ * stride + id];
-    return r;
-}
 
 // Jet boundary of step `step`: blockIdx.z == 0 is the inlet (y=0 plane), 1 the
 // outlet (y=NY-1 plane), unless `which` selects one.  Values go to the ghost
@@ -2841,8 +2843,14 @@ cudaError_t fused_configure(int smem) {
     return fused_attr<CodecF16, true, true>(smem);
 }
 
-cudaError_t launch_fused(const DeviceState &s, const FusedTiling &t, int cur, int64_t step, bool stats,
+cudaError_t launch_fused(const DeviceState &s, const FusedTiling &t_in, int cur, int64_t step, bool stats,
                          cudaStream_t st) {
+    FusedTiling t = t_in;
+    if (t.boundary) {
+        t.bnd_dst = s.pops[cur ^ 1];
+        t.bnd_psi = s.psi[(step + 1) & 1];
+        t.bnd_step = step;
+    }
     if (s.g.storage == kStoreF16)
         return stats ? fused_dispatch<CodecF16, true>(s, t, cur, step, st)
                      : fused_dispatch<CodecF16, false>(s, t, cur, step, st);

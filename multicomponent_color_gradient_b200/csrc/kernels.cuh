@@ -89,6 +89,11 @@ struct FusedTiling {
     int bulk;      // the pipelined march with rows staged by bulk copies (k_fused_bulk)
     int wait_limit;  // k_fused_bulk: tries (about 1 us each) of a wait for a staged row before it gives up
     int boundary;    // jet: the fused step writes the inlet and outlet columns itself (no k_boundary launch)
+    // set by launch_fused for each launch when `boundary`: the buffer the step
+    // writes, the next step's psi and the step (read only by the boundary rows)
+    void *bnd_dst;
+    float *bnd_psi;
+    long long bnd_step;
 };
 
 // Tries of a k_fused_bulk wait by default (about a second), and of the wait
