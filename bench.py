@@ -204,7 +204,8 @@ def adjoint_cost(steps: int, snapshots: int):
         T.step(steps)
         fr, fb = T.get_populations()
         rr, rb = fr.reshape(27, -1).sum(0, dtype=np.float64), fb.reshape(27, -1).sum(0, dtype=np.float64)
-        P.target = ((rr - rb) / (rr + rb)).astype(np.float32)
+        # psi of the target run; ghost nodes (no populations) enter no sum and stay 0
+        P.target = np.divide(rr - rb, rr + rb, out=np.zeros_like(rr), where=(rr + rb) > 0).astype(np.float32)
         P.evaluate(a)  # warm-up
         r = P.evaluate(a)
         S = P.solver(P.case["sigma"], P.case["taub"])
