@@ -315,7 +315,10 @@ mcg_status mcg_adjoint_run(mcg_handle *h, const float *psi_target, int32_t nstep
  * 48 B per node and step) and runs nsteps forward steps; with 0 < segment <
  * nsteps it keeps a snapshot (populations and outlet state, 216 B per node)
  * every `segment` steps and the tape of one segment, and runs about
- * 2*nsteps forward steps.  The forward states keep the handle's storage: with
+ * 2*nsteps forward steps.  When device memory allows more segment tapes
+ * (mcg_set_jet_adjoint_tapes), the first forward pass also records the last
+ * segments it runs through, and those are reversed without running them
+ * again.  The forward states keep the handle's storage: with
  * MCG_STORAGE_F16 the sweep is the float32 adjoint of the step taken at the
  * float16-stored forward states (snapshots then take 108 B per node).  The
  * handle's state is left as it was. */
@@ -355,6 +358,10 @@ mcg_status mcg_adjoint_plan_taped(int32_t nsteps, int32_t snapshots, int32_t tap
 /* Records of the taped segments of mcg_adjoint_run (default 20; 0: plain
  * treeverse, every op forming its record with the moments kernel). */
 mcg_status mcg_set_adjoint_tape(mcg_handle *h, int32_t records);
+/* Segment tapes of mcg_adjoint_jet_run / mcg_adjoint_jet_profile_run (each
+ * segment * ~48 B per node): 0 (default) as many as fit while 5 % of device
+ * memory (at least 4 GiB) stays free, n > 0 at most n.  One is always kept. */
+mcg_status mcg_set_jet_adjoint_tapes(mcg_handle *h, int32_t tapes);
 
 /* ---------------- output files (io/save_data.cuh, meanF/meanFieldsRT.cuh) ---------------- */
 

@@ -96,6 +96,7 @@ SIGNATURES = {
     "mcg_adjoint_plan": [C.c_int32, C.c_int32, C.POINTER(C.c_int64), _I32],
     "mcg_adjoint_plan_taped": [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int64), _I32],
     "mcg_set_adjoint_tape": [_P, C.c_int32],
+    "mcg_set_jet_adjoint_tapes": [_P, C.c_int32],
     "mcg_adjoint_jet_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _D, _D, C.POINTER(C.c_int64),
                             _F],
     "mcg_adjoint_jet_profile_run": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _F, _F, C.c_int32, _D,

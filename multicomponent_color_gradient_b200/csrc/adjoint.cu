@@ -279,6 +279,15 @@ mcg_status mcg_adjoint_plan(int32_t nsteps, int32_t snapshots, int64_t *forward_
     return mcg_adjoint_plan_taped(nsteps, snapshots, 0, forward_steps, sweeps);
 }
 
+mcg_status mcg_set_jet_adjoint_tapes(mcg_handle *h, int32_t tapes) {
+    return mcg::guarded([&]() -> mcg_status {
+        if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
+        if (tapes < 0) return fail(MCG_ERR_INVALID_ARG, "tapes must be >= 0");
+        h->jet_adjoint_tapes = tapes;
+        return MCG_OK;
+    });
+}
+
 mcg_status mcg_set_adjoint_tape(mcg_handle *h, int32_t records) {
     return mcg::guarded([&]() -> mcg_status {
         if (!h) return fail(MCG_ERR_INVALID_ARG, "handle is null");
@@ -488,9 +497,6 @@ mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t
         ADJ_CUDA(buf.alloc(&p, 5 * NP * sizeof(float)), "jet adjoint snapshots");
         snapB[size_t(j)] = static_cast<float *>(p);
     }
-    float *tape = nullptr;
-    ADJ_CUDA(buf.alloc(&p, size_t(L) * rec_floats * sizeof(float)), "jet adjoint moment tape");
-    tape = static_cast<float *>(p);
     float *lam[2];
     for (int k = 0; k < 2; ++k) {
         ADJ_CUDA(buf.alloc(&p, lam_bytes), "jet adjoint lambda buffers");
@@ -519,6 +525,26 @@ mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t
     if (profile) {
         ADJ_CUDA(buf.alloc(&p, M * sizeof(float)), "jet adjoint profile source");
         table = static_cast<float *>(p);
+    }
+    // segment tapes, allocated last: tapes[0] serves every segment pass 2
+    // re-runs; with more, pass 1 also records the last segments it runs
+    // through into tapes[1..] (segment nseg-1-k into tapes[k]), and pass 2
+    // reverses those without re-running them.  As many as fit with a margin
+    // of device memory left free (h->jet_adjoint_tapes == 0), or that many.
+    const size_t tape_bytes = size_t(L) * rec_floats * sizeof(float);
+    int64_t ntapes = 1;
+    {
+        size_t free_b = 0, total_b = 0;
+        ADJ_CUDA(cudaMemGetInfo(&free_b, &total_b), "device memory");
+        const size_t margin = std::max<size_t>(size_t(4) << 30, total_b / 20);
+        const int64_t fit = free_b > margin ? int64_t((free_b - margin) / tape_bytes) : 0;
+        const int64_t want = h->jet_adjoint_tapes > 0 ? int64_t(h->jet_adjoint_tapes) : nseg;
+        ntapes = std::max<int64_t>(1, std::min<int64_t>({want, nseg, fit}));
+    }
+    std::vector<float *> tapes(size_t(ntapes), nullptr);
+    for (int64_t k = 0; k < ntapes; ++k) {
+        ADJ_CUDA(buf.alloc(&p, tape_bytes), "jet adjoint moment tape");
+        tapes[size_t(k)] = static_cast<float *>(p);
     }
 
     const int64_t step0 = h->step;
@@ -557,8 +583,14 @@ mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t
     // at least through the window here, accumulating its radial statistics
     if (mcg_status st = save(0, 0)) return st;
     const int64_t pass1 = profile ? std::max<int64_t>(int64_t(t_end) + 1, (nseg - 1) * L) : (nseg - 1) * L;
+    auto pass1_tape = [&](int64_t j) -> float * {  // segment j's pass-1 tape, or none
+        const int64_t k = nseg - 1 - j;
+        return k >= 0 && k < ntapes ? tapes[size_t(k)] : nullptr;
+    };
     for (int64_t t = 0; t < pass1; ++t) {
-        if (mcg_status st = forward(t, nullptr, profile && t >= t_begin && t <= t_end)) return st;
+        float *seg = pass1_tape(t / L);
+        float *rec = seg ? seg + size_t(t - (t / L) * L) * rec_floats : nullptr;
+        if (mcg_status st = forward(t, rec, profile && t >= t_begin && t <= t_end)) return st;
         if ((t + 1) % L == 0 && (t + 1) / L < nseg)
             if (mcg_status st = save((t + 1) / L, t + 1)) return st;
     }
@@ -581,12 +613,18 @@ mcg_status jet_adjoint(mcg_handle *h, int32_t nsteps, int32_t t_begin, int32_t t
     int lc = 0, lb = 0;
     for (int64_t j = nseg - 1; j >= 0; --j) {
         const int64_t s0 = j * L, s1 = std::min<int64_t>(nsteps, s0 + L);
-        ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], state_bytes, cudaMemcpyDeviceToDevice, h->stream),
-                 "restore snapshot");
-        ADJ_LAUNCH(h, mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
-                   "jet adjoint: restore outlet");
-        for (int64_t t = s0; t < s1; ++t)
-            if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats, false)) return st;
+        float *tape = pass1_tape(j);
+        if (!tape || pass1 < s1) {  // not recorded whole in pass 1: restore and re-run into tapes[0]
+            tape = tapes[0];
+            ADJ_CUDA(cudaMemcpyAsync(work[s0 & 1], snap[size_t(j)], state_bytes, cudaMemcpyDeviceToDevice,
+                                     h->stream),
+                     "restore snapshot");
+            ADJ_LAUNCH(h,
+                       mcg::launch_restore_outlet_state(run, snapB[size_t(j)], run.psi[(step0 + s0) & 1], h->stream),
+                       "jet adjoint: restore outlet");
+            for (int64_t t = s0; t < s1; ++t)
+                if (mcg_status st = forward(t, tape + size_t(t - s0) * rec_floats, false)) return st;
+        }
         for (int64_t t = s1 - 1; t >= s0; --t) {
             const float *rec = tape + size_t(t - s0) * rec_floats;
             const bool in_window = t >= t_begin && t <= t_end;

@@ -39,6 +39,7 @@ struct mcg_handle {
     // radial statistics (meanF/memoryMeanFields.cuh:39-45)
     int stats_mode = -1;  // -1 automatic from NSTATS_START_STEP, 0 off, 1 on
     int adjoint_tape = 20;  // moment records the periodic adjoint's innermost segments tape (mcg_set_adjoint_tape)
+    int jet_adjoint_tapes = 0;  // segment tapes of the jet adjoint (0: as many as device memory allows)
     bool stats_started = false;
     uint32_t stats_start_step = 0;
     uint32_t stats_samples = 0;

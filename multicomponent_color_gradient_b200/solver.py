@@ -114,6 +114,11 @@ class Solver:
         assert all(a.size == self.N for a in arrs)
         self._c("mcg_init_equilibrium", *[_fptr(a) for a in arrs])
 
+    def set_jet_adjoint_tapes(self, tapes: int) -> None:
+        """Segment tapes of the jet adjoints (mcg_set_jet_adjoint_tapes; 0: as
+        many as device memory allows)."""
+        self._c("mcg_set_jet_adjoint_tapes", int(tapes))
+
     def adjoint_jet_run(self, nsteps: int, t_begin: int, t_end: int, y_obs: int, segment: int = 0) -> Dict:
         """J = sum over steps t_begin..t_end of (1/2) sum_{y >= y_obs} uy^2 and
         dJ/dc of the inlet-profile coefficients (8 values), from one forward +

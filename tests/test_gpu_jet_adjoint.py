@@ -90,13 +90,20 @@ def test_dJ_dc_matches_fp64_central_differences(adjoint, k):
 
 
 @pytest.mark.parametrize("segment", [7, 16])
-def test_segments_give_the_same_gradients(adjoint, segment):
+@pytest.mark.parametrize("tapes", [1, 3])
+def test_segments_give_the_same_gradients(adjoint, segment, tapes):
+    """Snapshots every `segment` steps, one segment tape (every segment re-run
+    once from its snapshot) or three (the two last segments of the first pass,
+    which stops before the last one, reversed from their pass-1 tapes): the
+    gradients of the all-steps tape."""
     with Solver(CASE) as S:
         S.set_inlet_bessel(C0.astype(np.float32))
         S.init_jet()
+        S.set_jet_adjoint_tapes(tapes)
         r = S.adjoint_jet_run(T, T0, T1, YOBS, segment=segment)
     nseg = -(-T // segment)
-    assert r["forward_steps"] == (nseg - 1) * segment + T
+    rerun = T - (min(tapes, nseg) - 1) * segment  # segments nseg-2 .. nseg-tapes come from pass 1
+    assert r["forward_steps"] == (nseg - 1) * segment + rerun
     assert abs(r["J"] - adjoint["J"]) <= 1e-12 * adjoint["J"]
     np.testing.assert_allclose(r["dJ_dc"], adjoint["dJ_dc"], rtol=1e-9, atol=1e-15)
 

@@ -124,11 +124,18 @@ def test_profile_dJ_dc_matches_fp64_central_differences(adjoint, target, k):
     assert abs(g - fd) <= 1e-3 * abs(fd), (k, g, fd)
 
 
-def test_profile_segments_give_the_same_gradients(adjoint, target):
+@pytest.mark.parametrize("tapes", [1, 2])
+def test_profile_segments_give_the_same_gradients(adjoint, target, tapes):
+    """Snapshots every 48 steps (segments of 48, 48, 48, 16).  The first pass
+    runs through the window's end, the last step, so the last `tapes` segments
+    are recorded there and only the others are re-run."""
     with Solver(case()) as S:
         S.set_inlet_bessel(C0.astype(np.float32))
         S.init_jet()
+        S.set_jet_adjoint_tapes(tapes)
         r = S.adjoint_jet_profile_run(T, T0, T1, Y_LO, Y_HI, target[0], target[1], segment=48)
+    lengths = [48, 48, 48, 16]
+    assert r["forward_steps"] == T + sum(lengths[:len(lengths) - tapes])
     assert abs(r["J"] - adjoint["J"]) <= 1e-12 * adjoint["J"]
     np.testing.assert_allclose(r["dJ_dc"], adjoint["dJ_dc"], rtol=1e-6, atol=1e-15)
 
