@@ -228,9 +228,10 @@ def jet_adjoint_cost(steps: int, segment: int, storage: str):
     J = the misfit of the time-averaged centreline velocity and half-width over
     the second half of the run for 2 <= y/D <= 10, against the profiles of a
     run with the coefficients perturbed by N(0, 0.05); forward states stored in
-    `storage`, float32 adjoint, a snapshot every `segment` steps.  Device time
-    of one sweep against `steps` plain forward steps of the same storage (and
-    of float32 storage)."""
+    `storage`, float32 adjoint, a snapshot every `segment` steps, as many
+    segment tapes as device memory allows (the library's default).  Device
+    time of one sweep against `steps` plain forward steps of the same storage
+    (and of float32 storage)."""
     import numpy as np
 
     from multicomponent_color_gradient_b200 import Solver, get_case
