@@ -1173,8 +1173,14 @@ __global__ void __launch_bounds__(kFusedThreads, PipeBlocks<C>::value) k_fused_p
             const float *mc = msm + ((c + kPipeStage) % kPipeStage) * mplane;
             // rows of this thread: pull rows lr, lr+rpt, ... (< ty+2) and relax rows
             // 1+lr, 1+lr+rpt, ... (<= ty), interleaved so that a warp has loads of
-            // one row in flight while it relaxes another
-            for (int r = lr; r < ty + 2; r += rpt) {
+            // one row in flight while it relaxes another.  With one row group (rows
+            // of 256 columns) the upper half of the row's threads takes the rows in
+            // a rotated order, so that one half pulls while the other relaxes, as
+            // two row groups do; the order of the rows within an iteration is free.
+            // (split at a warp boundary: the statistics are warp-collective)
+            const int rot = (rpt == 1 && x >= (tpr / 64) * 32) ? (ty + 2) / 2 : 0;
+            for (int ri = lr; ri < ty + 2; ri += rpt) {
+                const int r = rot ? (ri + rot) % (ty + 2) : ri;
                 const bool own = own_plane && r >= 1 && r <= ty;
                 const int rc = r + 1;
                 if constexpr (kOverlap) {
@@ -2758,11 +2764,16 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     const int per_row = t.tpr * 4;
     const int rpt = kFusedThreads / t.tpr;
     if (const char *v = std::getenv("MCG_FUSED_SMEM_KB")) max_smem = std::atoi(v) * 1024;  // tuning sweeps
-    // software-pipelined march for rows of up to 128 columns (4-row tiles at
-    // two CTAs per SM; measured on 128x256x128: +5 % float32, and +2 % float16
-    // with its loads in flight across the relaxation).  Rows of 256 columns
-    // need 2-row tiles: the block-synchronous march measured faster there.
+    // software-pipelined march for rows of up to 128 columns (measured on
+    // 128x256x128: +5 % float32, and +2 % float16 with its loads in flight
+    // across the relaxation)
     t.pipe = t.tpr <= 128;
+    // rows of 256 columns in float32 too, where one row group's upper half
+    // takes the rows in a rotated order (measured on 256x512x256: +2.4 % over
+    // the block-synchronous march at 32-plane chunks; float16 keeps the
+    // block-synchronous march, 16853 vs 16434 MLUPS)
+    const bool pipe256 = t.tpr == 256 && g.storage == kStoreF32;
+    if (pipe256) t.pipe = 1;
     if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v) != 0;  // tuning sweeps
     if (t.pipe) max_smem = std::max(max_smem, 112 * 1024);  // 4 ring + 3 stage planes: two CTAs per SM
     // rows per tile: at least one round of rows in parallel, 4 by default
@@ -2797,7 +2808,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
         // chunks keep the block-synchronous march, whose shorter chunks fill
         // the GPU.
         const int ctas16 = t.ny_tiles * ((g.NZ - 2 + 15) / 16);
-        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = g.storage == kStoreF16 ? 10 : 13;
+        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = pipe256 ? 32 : (g.storage == kStoreF16 ? 10 : 13);
         else if (!std::getenv("MCG_FUSED_PIPE")) t.pipe = 0;
     }
     if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
