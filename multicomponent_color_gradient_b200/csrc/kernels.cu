@@ -2769,9 +2769,11 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     // across the relaxation)
     t.pipe = t.tpr <= 128;
     // rows of 256 columns in float32 too, where one row group's upper half
-    // takes the rows in a rotated order (measured on 256x512x256: +2.4 % over
-    // the block-synchronous march at 32-plane chunks; float16 keeps the
-    // block-synchronous march, 16853 vs 16434 MLUPS)
+    // takes the rows in a rotated order, on 1-row tiles at 3 CTAs per SM
+    // (measured on 256x512x256: 11236 MLUPS at 24-plane chunks, against 10582
+    // on 2-row tiles at 2 CTAs per SM and 10336 for the block-synchronous
+    // march; float16 keeps the block-synchronous march on 2-row tiles, 16721
+    // against 13171 pipelined)
     const bool pipe256 = t.tpr == 256 && g.storage == kStoreF32;
     if (pipe256) t.pipe = 1;
     if (const char *v = std::getenv("MCG_FUSED_PIPE")) t.pipe = std::atoi(v) != 0;  // tuning sweeps
@@ -2783,6 +2785,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
     // the float32 pipelined march runs 3 CTAs per SM (PipeBlocks) on one round
     // of rows (2 rows for 128 columns; measured +1.5 % over 4-row tiles at 2 CTAs)
     if (t.pipe && g.storage == kStoreF32) ty = std::max(2, rpt);
+    if (t.pipe && pipe256) ty = 1;
     if (const char *v = std::getenv("MCG_FUSED_TY")) ty = std::max(1, std::atoi(v));  // tuning sweeps
     auto smem_of = [&](int h) {
         return (t.pipe ? kPipeRing * (h + 2) + kPipeStage * kMomCount * h : 3 * (h + 2) + 2 * kMomCount * h) * per_row;
@@ -2808,7 +2811,7 @@ FusedTiling fused_tiling(const Geometry &g, int max_smem) {
         // chunks keep the block-synchronous march, whose shorter chunks fill
         // the GPU.
         const int ctas16 = t.ny_tiles * ((g.NZ - 2 + 15) / 16);
-        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = pipe256 ? 32 : (g.storage == kStoreF16 ? 10 : 13);
+        if (ctas16 >= 3 * 148 && !std::getenv("MCG_FUSED_LZ")) lz = pipe256 ? 24 : (g.storage == kStoreF16 ? 10 : 13);
         else if (!std::getenv("MCG_FUSED_PIPE")) t.pipe = 0;
     }
     if (const char *v = std::getenv("MCG_FUSED_LZ")) lz = std::max(1, std::atoi(v));  // tuning sweeps
