@@ -4,9 +4,11 @@
   2000 steps): the float32 solver against the float64 oracle from the same
   seeded state (max |d psi| <= 1e-3, Laplace jump within 2 %, spurious-current
   peak within 5 %), and Laplace's law dp * R_eff constant across radii.
-* Float16 storage: the 64x128x64 jet crop (D=8, tau 0.52, sigma 0.005) run in
-  float32 and float16 storage against the float64 oracle; the radial mean
-  centre-line velocity and half-width agree within 1 % (the bar float16 storage is held to).
+* Float16 storage: the 64x128x64 jet crop run in float32 and float16 storage
+  against the float64 oracle, at D=8 (y/D = 2..6 inside the crop) and at the
+  256x512x256 jet's D=32 (Re 240, We 16: the same tau 0.52 and sigma 0.005;
+  y/D = 1..3); the radial mean centre-line velocity and half-width agree
+  within 1 % (the bar float16 storage is held to).
 """
 import numpy as np
 import pytest
@@ -120,29 +122,58 @@ def bin_centres(case):
     return out
 
 
+# Crop runs: (diameter D, steps, statistics from, rows as multiples of D).
+# D=8 is the crop scaled with the domain; D=32 keeps the 256x512x256 jet's
+# own diameter (Re 240, We 16 give the same tau 0.52 and sigma 0.005), so the
+# crop holds y/D <= 4 and the jet fills half the lateral width.
+CROPS = {
+    8: dict(steps=1200, stats_from=600, overrides={}, ks=(2, 3, 4, 5, 6)),
+    32: dict(steps=2400, stats_from=1200, overrides=dict(jet_radius=16.0, Re=240.0, We=16.0), ks=(1, 2, 3)),
+}
+_crop_oracle = {}
+
+
+def _crop_case(D, **kw):
+    c = CROPS[D]
+    return get_case("jet_64x128x64", NSTATS_START_STEP=c["stats_from"], **c["overrides"], **kw)
+
+
+def _crop_oracle_run(D):
+    """The float64 oracle's radial statistics and fields of crop D (one run
+    shared by both storages)."""
+    if D not in _crop_oracle:
+        O = Oracle(_crop_case(D), 64)
+        O.init_jet()
+        O.step(CROPS[D]["steps"])
+        _crop_oracle[D] = (O.get_radial(), O.get_fields())
+    return _crop_oracle[D]
+
+
+@pytest.mark.parametrize("D", [8, 32])
 @pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_jet_crop_profiles_within_one_percent_of_fp64(storage):
-    steps, stats_from = 1200, 600
-    case = get_case("jet_64x128x64", storage=storage, NSTATS_START_STEP=stats_from)
+def test_jet_crop_profiles_within_one_percent_of_fp64(storage, D):
+    case = _crop_case(D, storage=storage)
+    assert 2 * case["jet_radius"] == D
+    if D == 32:
+        assert abs(case["taur"] - 0.52) < 1e-6 and abs(case["sigma"] - 0.005) < 1e-6, (case["taur"], case["sigma"])
     S = Solver(case)
     S.init_jet()
-    S.step(steps)
-    O = Oracle(get_case("jet_64x128x64", NSTATS_START_STEP=stats_from), 64)
-    O.init_jet()
-    O.step(steps)
+    S.step(CROPS[D]["steps"])
+    OR, OF = _crop_oracle_run(D)
     NY, NRB = case["NY"], case["NX"] // 2
-    U, OU = radial_mean_uy(S.get_radial(), NY, NRB), radial_mean_uy(O.get_radial(), NY, NRB)
+    U, OU = radial_mean_uy(S.get_radial(), NY, NRB), radial_mean_uy(OR, NY, NRB)
     radius = bin_centres(case)
-    D = 2 * case["jet_radius"]
-    rows = [int(round(k * D)) for k in (2, 3, 4, 5, 6)]  # y/D = 2..6 inside the 128-long crop
+    rows = [int(round(k * D)) for k in CROPS[D]["ks"]]
     for y in rows:
         uc, ouc = U[y, 0], OU[y, 0]
-        assert abs(uc - ouc) <= 0.01 * abs(ouc), (storage, y, uc, ouc)
+        assert abs(uc - ouc) <= 0.01 * abs(ouc), (storage, D, y, uc, ouc)
         hw, ohw = half_width(U[y], radius), half_width(OU[y], radius)
         if np.isfinite(ohw):
-            assert abs(hw - ohw) <= 0.01 * ohw, (storage, y, hw, ohw)
-    F, OF = S.get_fields(), O.get_fields()
+            assert abs(hw - ohw) <= 0.01 * ohw, (storage, D, y, hw, ohw)
+        print(f"{storage} D={D} y/D={y / D:.0f}: u_c {uc:.6f} (fp64 {ouc:.6f}), r_half {hw:.4f} (fp64 {ohw:.4f})")
+    F = S.get_fields()
+    S.close()
     m = interior(case)
     dpsi = maxabs(psi_of(F["rhor"][m], F["rhob"][m]), psi_of(OF["rhor"][m], OF["rhob"][m]))
-    print(f"{storage}: max|d psi| vs fp64 = {dpsi:.3e}")
+    print(f"{storage} D={D}: max|d psi| vs fp64 = {dpsi:.3e}")
     assert dpsi <= (1e-3 if storage == "f32" else 2e-2)
