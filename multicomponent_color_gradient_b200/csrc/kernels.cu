@@ -1673,8 +1673,12 @@ __global__ void k_init_fields(const DeviceState s, int mode, int red_inside, flo
     for (int k = kMomUX; k < kMomCount; ++k) s.mom[size_t(k) * N + id] = 0.0f;
 }
 
-// Populations of every interior node, written at their pull sources in both
-// buffers (so slots no kernel rewrites hold the initial value in both).
+// Populations of every interior node, written at their pull sources.  The
+// current buffer takes every slot; the other one only the slots on a y ghost
+// plane, which no step rewrites (they must hold the initial value in both
+// buffers).  Every other slot of the other buffer is written by the first
+// step before anything reads it.  Directions are unrolled, so the pull
+// source and the equilibrium take compile-time lattice constants.
 template <class C>
 __global__ void k_init_pops(const DeviceState s, int mode, float noise) {
     const Geometry &g = s.g;
@@ -1687,21 +1691,23 @@ __global__ void k_init_pops(const DeviceState s, int mode, float noise) {
     const float rr = s.mom[kMomRR * N + id], rb = s.mom[kMomRB * N + id];
     const float ux = s.mom[kMomUX * N + id], uy = s.mom[kMomUY * N + id], uz = s.mom[kMomUZ * N + id];
     const float usq = ux * ux + uy * uy + uz * uz;
-    for (int i = 0; i < kQ; ++i) {
+    const bool periodic = g.boundary == kBoundaryPeriodic;
+    static_for<kQ>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        using D = Dir<i>;
         float fr, fb;
         if (mode == 3) {
             // per colour, the third-order equilibrium at the node's velocity (lbm.cuh:16-35)
-            const float cu = float(dir_cx(i)) * ux + float(dir_cy(i)) * uy + float(dir_cz(i)) * uz;
+            const float cu = D::fx * ux + D::fy * uy + D::fz * uz;
             const float A2 = (cu * cu) * kInv2Cs4 - usq * kInv2Cs2 + cu * kInvCs2;
             const float A3 = cu * ((cu * cu) * kInv6Cs6 - usq * kInv2Cs4);
-            const float e = dir_w(i) * (1.0f + A2 + A3);
+            const float e = D::w * (1.0f + A2 + A3);
             fr = e * rr;
             fb = e * rb;
         } else {
             // jetDensity: feq(rho, 0) = w rho; bubble: w rho (jetIn.cuh:26-34, bubbleIn.cuh:25-39)
-            const float w = dir_w(i);
-            fr = w * rr;
-            fb = w * rb;
+            fr = D::w * rr;
+            fb = D::w * rb;
             if (noise != 0.0f) {
                 const float u = hash_uniform(s.ph.seed, 0x1D17ull, id, uint64_t(i));
                 const float f = 1.0f + (2.0f * u - 1.0f) * noise;
@@ -1712,8 +1718,8 @@ __global__ void k_init_pops(const DeviceState s, int mode, float noise) {
         int xs, ys, zs;
         pull_src_rt(g, x, y, z, i, xs, ys, zs);
         C::store_to(s.pops[0], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
-        C::store_to(s.pops[1], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
-    }
+        if (!periodic && (ys == 0 || ys == g.NY - 1)) C::store_to(s.pops[1], g, i, xs, ys, zs, fr, fb, s.ph.f16_rho0);
+    });
 }
 
 __global__ void k_refresh_psi(const DeviceState s) {
