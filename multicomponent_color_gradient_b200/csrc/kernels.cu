@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "kernels.cuh"
 #include "lattice.cuh"
@@ -152,10 +153,18 @@ struct CodecF16 {
     // difference d = fr - fb.  With q the signed minority fraction, fr - fb =
     // g (1 - q) when red is the majority and -g (1 + q) otherwise, i.e.
     // g (sign(q) - q).
+    // The read-only load asks L2 to fetch 256-byte blocks on a miss: the words
+    // of a pulled row segment are then in L2 for the neighbouring warps'
+    // loads (measured +0.3 % on the 128x256x128 jet, +1.2 % on 256-column
+    // rows; no change in float32).
     using Raw = __half2;
     template <int I>
     __device__ __forceinline__ Raw load_raw(const __half2 *p) const {
-        return __ldg(p);
+        uint32_t u;
+        asm("ld.global.nc.L2::256B.b32 %0, [%1];" : "=r"(u) : "l"(p));
+        __half2 h;
+        memcpy(&h, &u, sizeof h);
+        return h;
     }
     template <int I>
     __device__ __forceinline__ float2 decode(Raw h, float &gi) const {
